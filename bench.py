@@ -1,0 +1,300 @@
+"""Benchmark: Fock builds/s for C60/6-31G(d) on one B200.
+
+One step = one full Fock build at a fixed density: fock_build_diag +
+fock_build_non_diag at thr = 1e-10 (the reference's definition of a build,
+direct_hartreefock.f90:106-110), excluding the once-per-SCF set-up
+(hfgpu_init + fock_build_initial_diag).
+
+  value   device-resident builds/s (F, P in HBM; hfgpu_fock_build_device)
+  e2e     the same build through the reference-facing C ABI with HOST
+          buffers (fock_build_diag + fock_build_non_diag, H2D/D2H included)
+  roofline  the dominant quartet-class kernel against the measured FP64 FMA
+          peak of the device
+  cpu_baseline  the CPU oracle (a restatement of the reference's Fortran) on
+          the host cores, on a bounded row sample of the same build
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+Under torchrun each rank runs an independent replica on its own GPU (the
+builder is single-GPU by design); value is the sum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Fock builds/s, C60/6-31G(d)"
+THR = 1e-10
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--molecule", default="c60")
+    ap.add_argument("--density", default="huckel", choices=["huckel", "guess"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload(name: str, density: str):
+    from hfcode_b200 import basis, molecules, onee
+    if name == "c60":
+        mol, bas = molecules.c60(), basis.load_basis("6-31G(d)")
+        label = "C60/6-31G(d)"
+    elif name == "benzene":
+        mol, bas = molecules.benzene(), basis.load_basis("6-31G(d)")
+        label = "benzene/6-31G(d)"
+    else:
+        n = int(name[1:name.index("h")])
+        mol, bas = molecules.alkane(n), basis.load_basis("6-31G(d)")
+        label = f"C{n}H{2 * n + 2}/6-31G(d)"
+    sh = basis.spread_basis(mol, bas)
+    if density == "guess":
+        p = basis.density_superposition(mol, bas, sh.nb)
+    else:
+        p = onee.huckel_density(mol, sh)
+    return label, mol, sh, p
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for n, v in zip(names, r[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+            except Exception:
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(sh, p, target_s: float, n_pass_total: int):
+    """Oracle (reference restatement) on the host cores, bounded row sample."""
+    from oracle import pyoracle
+    orc = pyoracle.Oracle(sh)
+    nb = sh.nb
+    f = np.zeros((nb, nb))
+    orc.fock_build_initial_diag(f, p, THR)
+    t0 = time.perf_counter()
+    orc.fock_build_diag(f, p, THR)
+    t_diag = time.perf_counter() - t0
+    stride = 4096
+    while True:
+        t0 = time.perf_counter()
+        n = orc.fock_build_non_diag_sample(f, p, THR, stride, 0)
+        dt = time.perf_counter() - t0
+        if dt > 0.3 * target_s or stride == 1:
+            break
+        stride = max(1, int(stride * max(0.05, dt) / target_s))
+    t_full = t_diag + dt * (n_pass_total / max(n, 1))
+    threads = pyoracle.lib().orc_num_threads()
+    return {"value": 1.0 / t_full, "unit": "builds/s", "cores": threads, "kind": "port",
+            "sample": f"bra rows ii % {stride} == 0 of every class block: {n} of {n_pass_total} screened-in "
+                      f"quartets in {dt:.1f} s, extrapolated by quartet count; diag part timed in full "
+                      f"({t_diag:.2f} s)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    label, mol, sh, p = workload(args.molecule, args.density)
+    # the screened-in quartet count of the full build, from the oracle's own
+    # screen on a full pass of the cheap diag + count-only sample scale
+    from oracle import pyoracle
+    orc = pyoracle.Oracle(sh)
+    f = np.zeros((sh.nb, sh.nb))
+    orc.fock_build_initial_diag(f, p, THR)
+    vals = []
+    samples = []
+    for it in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        orc.fock_build_diag(f, p, THR)
+        td = time.perf_counter() - t0
+        stride = max(1, int(os.environ.get("HF_REF_STRIDE", "64")))
+        t0 = time.perf_counter()
+        n = orc.fock_build_non_diag_sample(f, p, THR, stride, it % stride)
+        ts = time.perf_counter() - t0
+        if it >= args.warmup:
+            vals.append(1.0 / (td + ts * stride))
+            samples.append(n)
+    v = float(np.median(vals))
+    threads = pyoracle.lib().orc_num_threads()
+    cb = {"value": v, "unit": "builds/s", "cores": threads, "kind": "port",
+          "sample": f"each step: fock_build_diag in full + fock_build_non_diag on bra rows ii % {stride} == step "
+                    f"(~1/{stride} of the quartets), time x{stride}"}
+    print(json.dumps({"metric": METRIC, "value": v, "unit": "builds/s", "impl": "reference", "n_gpus": 0,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v,
+                      "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+                      "config": {"workload": f"{label} one Fock build (diag + non_diag), thr=1e-10",
+                                 "nb": sh.nb, "density": args.density},
+                      "cpu_baseline": cb,
+                      "e2e": {"value": v, "unit": "builds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    from hfcode_b200 import fock
+    from hfcode_b200.csrc import gen_eri  # noqa: F401  (flop table lives beside the generator)
+    label, mol, sh, p = workload(args.molecule, args.density)
+    nb = sh.nb
+    fb = fock.FockBuilder(sh)
+    # cycle-1 set-up: Schwarz factors (not timed)
+    f0 = np.zeros((nb, nb))
+    fb.fock_build_initial_diag(f0, p, THR)
+    dev = torch.device("cuda", local)
+    P = torch.from_numpy(np.ascontiguousarray(p)).to(dev)
+    F = torch.zeros((nb, nb), dtype=torch.float64, device=dev)
+    stream = torch.cuda.ExternalStream(fb.stream(), device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def step():
+        fb.fock_build_device(F.data_ptr(), P.data_ptr(), THR, THR, 0.0)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    times = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()  # L2 flush between timed steps (outside the events)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    total_ms = float(sum(times))
+    if dist:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    value = world * args.steps / (total_ms / 1000.0)
+    st = fb.class_stats()
+    n_pass = int(st["pass"].sum())
+    launches_per_step = 1 + 6 + 1 + int(np.count_nonzero(st["pass"])) + 1
+    # e2e through the reference-facing C ABI with host buffers
+    fh = np.zeros((nb, nb), order="F")
+    ph = np.ascontiguousarray(p)
+    fb.fock_build_diag(fh, ph, THR)
+    fb.fock_build_non_diag(fh, ph, THR)
+    e2e_t = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        fb.fock_build_diag(fh, ph, THR)
+        fb.fock_build_non_diag(fh, ph, THR)
+        e2e_t.append(time.perf_counter() - t0)
+    e2e = {"value": world * args.steps / sum(e2e_t), "unit": "builds/s",
+           "h2d_bytes_per_step": 2 * 2 * nb * nb * 8, "d2h_bytes_per_step": 2 * nb * nb * 8}
+    # instrumented step: per-class kernel times for the roofline
+    fb.set_timing(True)
+    step()
+    torch.cuda.synchronize()
+    st = fb.class_stats()
+    fb.set_timing(False)
+    flops_tab = json.load(open(os.path.join(ROOT, "hfcode_b200", "csrc", "generated", "class_flops.json")))
+    cls_flops = np.array([flops_tab[str(c)]["flops_prim"] * st["prim"][c] + flops_tab[str(c)]["flops_quartet"] *
+                          st["pass"][c] for c in range(21)], dtype=np.float64)
+    top = int(np.argmax(st["ms"]))
+    fp64_peak, fp32_peak = fock.measure_fma_peak()
+    achieved = cls_flops[top] / (st["ms"][top] * 1e-3) / 1e12
+    peak_tf = fp64_peak / 1e3
+    roof = {"bound": "fp64", "kernel": f"k_nondiag {fock.CLASS_NAMES[top]}", "achieved": achieved,
+            "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf, "traffic": None,
+            "peak_source": "measured FP64 FMA-chain probe on this device (MEASURED_PEAKS.json has no FP64 figure)",
+            "all_classes_tflops": float(cls_flops.sum() / (st["ms"].sum() * 1e-3) / 1e12),
+            "class_ms": {fock.CLASS_NAMES[c]: round(float(st["ms"][c]), 3) for c in range(21) if st["ms"][c] > 0}}
+    out = {"metric": METRIC, "value": value, "unit": "builds/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": f"{label} one Fock build (fock_build_diag + fock_build_non_diag), thr=1e-10",
+                      "nb": nb, "density": args.density, "parallelism": f"replicas{world}",
+                      "l2": "flushed between steps (256 MiB write outside the timed events)"},
+           "quartets_per_s": n_pass * value, "screened_in_quartets": n_pass,
+           "e2e": e2e, "gpu_launches": launches_per_step * args.steps, "roofline": roof,
+           "fp64_peak_tflops": peak_tf, "fp32_peak_tflops": fp32_peak / 1e3,
+           "clocks": clk.summary()}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(sh, p, args.cpu_seconds, n_pass)
+    if rank == 0:
+        print(json.dumps(out))
+    fb.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,368 @@
+// Shared device code of the B200 Fock builder: data layout, Boys function,
+// J/K scatter and the kernel templates instantiated once per quartet class
+// (one translation unit per class, see generated/cls_*.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <type_traits>
+
+namespace hfgpu {
+
+constexpr double INTTHRESH = 1e-10;     // molprops.f90:162
+constexpr int NPT = 6;                  // GPU pair types SS LS LL DS DL DD
+constexpr int NCLS = 21;                // quartet classes over the pair types
+constexpr int BOYS_NPT = 225;           // grid T_j = j/8, j = 0..224 (T <= 28)
+constexpr int BOYS_K = 8;               // Taylor terms per grid point
+constexpr int BOYS_MMAX = 8;            // highest order used: (dd|dd)
+
+// Primitive pair (one surviving primitive product of a shell pair): exponent
+// sum p, centre P, K_ab = sqrt(2 pi^2.5) exp(-ab/p r^2)/p d_a d_b
+// (precalc_kabs.f90:103-109) and the L-shell p/s ratios of both primitives.
+struct GPrim {
+    double p;
+    double P[3];
+    double K;
+    double w1, w2;
+    double pad;
+};
+
+// Shell pair in GPU orientation (larger shell first).
+struct GPair {
+    double A[3];
+    double B[3];
+    int p0, np;    // range in the primitive-pair array
+    int sa, sb;    // shell indices
+    int aoa, aob;  // first AO of each shell
+};
+
+// ---------------------------------------------------------------- Boys ----
+// F_m(T) for m = 0..M.  T > 28: F_0 = sqrt(pi/T)/2 and upward recursion
+// without the exponential, which is what the reference evaluates there
+// (boys.f90:134-139).  T <= 28: 8-term Taylor expansion of F_M about the
+// nearest point of a 1/8-spaced grid (coefficients F_{M+k}(T_j)(-1)^k/k!
+// staged in shared memory), then downward recursion
+// F_m = (2T F_{m+1} + e^-T)/(2m+1).
+template <int M>
+__device__ __forceinline__ void boys_eval(double T, const double* __restrict__ tab, double* F) {
+    if (T > 28.0) {
+        const double it = 1.0 / T;
+        F[0] = 0.88622692545275801365 * sqrt(it);
+#pragma unroll
+        for (int m = 1; m <= M; ++m) F[m] = F[m - 1] * ((m - 0.5) * it);
+    } else {
+        const int j = __double2int_rn(T * 8.0);
+        const double x = T - 0.125 * j;
+        const double* c = tab + j * BOYS_K;
+        double f = c[BOYS_K - 1];
+#pragma unroll
+        for (int k = BOYS_K - 2; k >= 0; --k) f = fma(f, x, c[k]);
+        F[M] = f;
+        if (M > 0) {
+            const double e = exp(-T);
+            const double t2 = T + T;
+#pragma unroll
+            for (int m = M - 1; m >= 0; --m) F[m] = fma(t2, F[m + 1], e) * (1.0 / (2 * m + 1));
+        }
+    }
+}
+
+template <int M>
+__device__ __forceinline__ void boys_eval(float T, const float* __restrict__ tab, float* F) {
+    if (T > 28.0f) {
+        const float it = 1.0f / T;
+        F[0] = 0.886226925f * sqrtf(it);
+#pragma unroll
+        for (int m = 1; m <= M; ++m) F[m] = F[m - 1] * ((m - 0.5f) * it);
+    } else {
+        const int j = __float2int_rn(T * 8.0f);
+        const float x = T - 0.125f * j;
+        const float* c = tab + j * BOYS_K;
+        float f = c[5];
+#pragma unroll
+        for (int k = 4; k >= 0; --k) f = fmaf(f, x, c[k]);
+        F[M] = f;
+        if (M > 0) {
+            const float e = __expf(-T);
+            const float t2 = T + T;
+#pragma unroll
+            for (int m = M - 1; m >= 0; --m) F[m] = fmaf(t2, F[m + 1], e) * (1.0f / (2 * m + 1));
+        }
+    }
+}
+
+
+// ------------------------------------------------------- class traits ----
+__host__ __device__ constexpr int pt_na(int t) { return t == 0 ? 1 : t == 1 ? 4 : t == 2 ? 4 : 5; }
+__host__ __device__ constexpr int pt_nb(int t) { return t == 0 ? 1 : t == 1 ? 1 : t == 2 ? 4 : t == 3 ? 1 : t == 4 ? 4 : 5; }
+
+#define HF_CLASS_TRAITS(ci, bi, ki, NAME, nout, L)                                                   \
+    struct Cls_##NAME {                                                                              \
+        static constexpr int CI = ci, BI = bi, KI = ki, NOUT = nout, LL = L;                         \
+        __device__ __forceinline__ static void eri(const GPair& b, const GPair& k, const GPrim* p,   \
+                                                   const double* t, double* o) {                     \
+            eri_##NAME(b, k, p, t, o);                                                               \
+        }                                                                                            \
+        __device__ __forceinline__ static void eri32(const GPair& b, const GPair& k, const GPrim* p,  \
+                                                     const float* t, float* o) {                     \
+            eri_##NAME##_f32(b, k, p, t, o);                                                         \
+        }                                                                                            \
+    };
+
+// ------------------------------------------------------------ scatter ----
+// F contributions of one shell quartet with uniform weight s, into the
+// one-triangle buffer G (F += G + G^T later).  Column-major P(r,c)=P[r+c*nb].
+template <int NA, int NB, int NC, int ND, typename E>
+__device__ __forceinline__ void scatter_quartet(const E* e, double s, int a0, int b0, int c0, int d0,
+                                                const double* __restrict__ P, double* __restrict__ G,
+                                                int nb, bool jonly) {
+    auto Pm = [&](int r, int c) { return __ldg(P + r + (size_t)c * nb); };
+    auto idx = [](int i, int j, int k, int l) { return ((i * NB + j) * NC + k) * ND + l; };
+    double pcd[NC * ND], pab[NA * NB];
+#pragma unroll
+    for (int k = 0; k < NC; ++k)
+#pragma unroll
+        for (int l = 0; l < ND; ++l) pcd[k * ND + l] = Pm(c0 + k, d0 + l);
+#pragma unroll
+    for (int i = 0; i < NA; ++i)
+#pragma unroll
+        for (int j = 0; j < NB; ++j) pab[i * NB + j] = Pm(a0 + i, b0 + j);
+    const double s2 = 2.0 * s;
+    // J_ab and J_cd
+#pragma unroll
+    for (int i = 0; i < NA; ++i)
+#pragma unroll
+        for (int j = 0; j < NB; ++j) {
+            double acc = 0.0;
+#pragma unroll
+            for (int k = 0; k < NC; ++k)
+#pragma unroll
+                for (int l = 0; l < ND; ++l) acc += pcd[k * ND + l] * (double)e[idx(i, j, k, l)];
+            atomicAdd(G + (a0 + i) + (size_t)(b0 + j) * nb, s2 * acc);
+        }
+#pragma unroll
+    for (int k = 0; k < NC; ++k)
+#pragma unroll
+        for (int l = 0; l < ND; ++l) {
+            double acc = 0.0;
+#pragma unroll
+            for (int i = 0; i < NA; ++i)
+#pragma unroll
+                for (int j = 0; j < NB; ++j) acc += pab[i * NB + j] * (double)e[idx(i, j, k, l)];
+            atomicAdd(G + (c0 + k) + (size_t)(d0 + l) * nb, s2 * acc);
+        }
+    if (jonly) return;
+    const double hs = -0.5 * s;
+    // K_ac (sum over j,l of P_jl), K_ad (P_jk), K_bc (P_il), K_bd (P_ik)
+    {
+        double pbd[NB * ND];
+#pragma unroll
+        for (int j = 0; j < NB; ++j)
+#pragma unroll
+            for (int l = 0; l < ND; ++l) pbd[j * ND + l] = Pm(b0 + j, d0 + l);
+#pragma unroll
+        for (int i = 0; i < NA; ++i)
+#pragma unroll
+            for (int k = 0; k < NC; ++k) {
+                double acc = 0.0;
+#pragma unroll
+                for (int j = 0; j < NB; ++j)
+#pragma unroll
+                    for (int l = 0; l < ND; ++l) acc += pbd[j * ND + l] * (double)e[idx(i, j, k, l)];
+                atomicAdd(G + (a0 + i) + (size_t)(c0 + k) * nb, hs * acc);
+            }
+    }
+    {
+        double pbc[NB * NC];
+#pragma unroll
+        for (int j = 0; j < NB; ++j)
+#pragma unroll
+            for (int k = 0; k < NC; ++k) pbc[j * NC + k] = Pm(b0 + j, c0 + k);
+#pragma unroll
+        for (int i = 0; i < NA; ++i)
+#pragma unroll
+            for (int l = 0; l < ND; ++l) {
+                double acc = 0.0;
+#pragma unroll
+                for (int j = 0; j < NB; ++j)
+#pragma unroll
+                    for (int k = 0; k < NC; ++k) acc += pbc[j * NC + k] * (double)e[idx(i, j, k, l)];
+                atomicAdd(G + (a0 + i) + (size_t)(d0 + l) * nb, hs * acc);
+            }
+    }
+    {
+        double pad_[NA * ND];
+#pragma unroll
+        for (int i = 0; i < NA; ++i)
+#pragma unroll
+            for (int l = 0; l < ND; ++l) pad_[i * ND + l] = Pm(a0 + i, d0 + l);
+#pragma unroll
+        for (int j = 0; j < NB; ++j)
+#pragma unroll
+            for (int k = 0; k < NC; ++k) {
+                double acc = 0.0;
+#pragma unroll
+                for (int i = 0; i < NA; ++i)
+#pragma unroll
+                    for (int l = 0; l < ND; ++l) acc += pad_[i * ND + l] * (double)e[idx(i, j, k, l)];
+                atomicAdd(G + (b0 + j) + (size_t)(c0 + k) * nb, hs * acc);
+            }
+    }
+    {
+        double pac[NA * NC];
+#pragma unroll
+        for (int i = 0; i < NA; ++i)
+#pragma unroll
+            for (int k = 0; k < NC; ++k) pac[i * NC + k] = Pm(a0 + i, c0 + k);
+#pragma unroll
+        for (int j = 0; j < NB; ++j)
+#pragma unroll
+            for (int l = 0; l < ND; ++l) {
+                double acc = 0.0;
+#pragma unroll
+                for (int i = 0; i < NA; ++i)
+#pragma unroll
+                    for (int k = 0; k < NC; ++k) acc += pac[i * NC + k] * (double)e[idx(i, j, k, l)];
+                atomicAdd(G + (b0 + j) + (size_t)(d0 + l) * nb, hs * acc);
+            }
+    }
+}
+
+// ------------------------------------------------------- kernel args ----
+struct ClassStats {
+    unsigned long long scattered, prim, fp32;
+};
+
+struct NDArgs {
+    const uint2* quartets;  // this class's list (fp64 from the front, fp32 from the back)
+    int n;                  // number of quartets to process
+    int from_back;          // 1: entry t is quartets[cap-1-t]
+    long long cap;
+    const GPair* bra;
+    const GPair* ket;
+    const GPrim* prims;
+    const double* boys;     // global table, [M][225][8]
+    const float* boysf;
+    const double* P;
+    double* G;
+    int nb;
+    double thr;
+    int jonly;
+    ClassStats* stats;
+};
+
+template <int M, typename T>
+__device__ __forceinline__ void stage_boys(T* sm, const T* g) {
+    const T* src = g + (size_t)M * BOYS_NPT * BOYS_K;
+    for (int i = threadIdx.x; i < BOYS_NPT * BOYS_K; i += blockDim.x) sm[i] = src[i];
+    __syncthreads();
+}
+
+__device__ __forceinline__ void warp_add_stats(ClassStats* st, unsigned long long sc, unsigned long long pr,
+                                               unsigned long long f32) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sc += __shfl_down_sync(0xffffffffu, sc, o);
+        pr += __shfl_down_sync(0xffffffffu, pr, o);
+        f32 += __shfl_down_sync(0xffffffffu, f32, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (sc) atomicAdd(&st->scattered, sc);
+        if (pr) atomicAdd(&st->prim, pr);
+        if (f32) atomicAdd(&st->fp32, f32);
+    }
+}
+
+constexpr int ND_THREADS = 128;
+
+template <class C, bool F32>
+__global__ void __launch_bounds__(ND_THREADS) k_nondiag(NDArgs a) {
+    using Real = typename std::conditional<F32, float, double>::type;
+    __shared__ Real sboys[BOYS_NPT * BOYS_K];
+    if constexpr (F32) stage_boys<C::LL>(sboys, a.boysf);
+    else stage_boys<C::LL>(sboys, a.boys);
+    constexpr int NA = pt_na(C::BI), NB = pt_nb(C::BI), NC = pt_na(C::KI), ND = pt_nb(C::KI);
+    static_assert(NA * NB * NC * ND == C::NOUT, "class size");
+    unsigned long long nsc = 0, npr = 0;
+    const int stride = gridDim.x * blockDim.x;
+    // every thread runs the same number of loop trips so the warp-level
+    // statistics reduction below sees all 32 lanes
+    const int trips = (a.n + stride - 1) / stride;
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int it = 0; it < trips; ++it, t += stride) {
+        if (t >= a.n) continue;
+        const uint2 q = a.from_back ? a.quartets[a.cap - 1 - t] : a.quartets[t];
+        const GPair bra = a.bra[q.x];
+        const GPair ket = a.ket[q.y];
+        Real e[C::NOUT];
+        if constexpr (F32) C::eri32(bra, ket, a.prims, sboys, e);
+        else C::eri(bra, ket, a.prims, sboys, e);
+        npr += (unsigned long long)(bra.np * ket.np);
+        Real mx = 0;
+#pragma unroll
+        for (int i = 0; i < C::NOUT; ++i) mx = fmax(mx, fabs(e[i]));
+        if ((double)mx < a.thr) continue;  // fock_build_non_diag.f90:69
+        ++nsc;
+        const double s = (bra.sa == bra.sb ? 0.5 : 1.0) * (ket.sa == ket.sb ? 0.5 : 1.0);
+        scatter_quartet<NA, NB, NC, ND>(e, s, bra.aoa, bra.aob, ket.aoa, ket.aob, a.P, a.G, a.nb, a.jonly);
+    }
+    if (a.stats) warp_add_stats(a.stats, nsc, npr, F32 ? nsc : 0ull);
+}
+
+struct DiagArgs {
+    const GPair* pairs;
+    int n;
+    const GPrim* prims;
+    const double* boys;
+    double* schw;          // mode 0: written; mode 1: read
+    const double* md;      // mode 1: nsh x nsh maxdm
+    int nsh;
+    const double* P;
+    double* G;
+    int nb;
+    double thr;
+};
+
+// Shell pairs with themselves, (ab|ab): fock_build_initial_diag.f90 (MODE 0)
+// and fock_build_diag.f90 (MODE 1).
+template <class C, int MODE>
+__global__ void __launch_bounds__(ND_THREADS) k_diag(DiagArgs a) {
+    __shared__ double sboys[BOYS_NPT * BOYS_K];
+    stage_boys<C::LL>(sboys, a.boys);
+    constexpr int NA = pt_na(C::BI), NB = pt_nb(C::BI);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.n) return;
+    const GPair pr = a.pairs[t];
+    if (MODE == 1) {
+        const double mv = fmax(a.md[pr.sa * a.nsh + pr.sb],
+                               fmax(0.25 * a.md[pr.sb * a.nsh + pr.sb], 0.25 * a.md[pr.sa * a.nsh + pr.sa]));
+        const double sw = a.schw[t];
+        if (sw * sw * mv < a.thr) return;  // fock_build_diag.f90:20-21
+    }
+    double e[C::NOUT];
+    C::eri(pr, pr, a.prims, sboys, e);
+    if (MODE == 0) {
+        double mx = 0;
+#pragma unroll
+        for (int i = 0; i < C::NOUT; ++i) mx = fmax(mx, fabs(e[i]));
+        a.schw[t] = sqrt(mx);
+    }
+#pragma unroll
+    for (int i = 0; i < C::NOUT; ++i)
+        if (!(fabs(e[i]) > INTTHRESH)) e[i] = 0.0;  // element skip
+    const double f = pr.sa == pr.sb ? 1.0 : 2.0;
+    scatter_quartet<NA, NB, NA, NB>(e, f * f / 8.0, pr.aoa, pr.aob, pr.aoa, pr.aob, a.P, a.G, a.nb, false);
+}
+
+
+typedef void (*NDKernel)(NDArgs);
+typedef void (*DiagKernel)(DiagArgs);
+
+// Kernels of one quartet class, filled by the class's translation unit.
+struct ClassKernels {
+    NDKernel nd64, nd32;
+    DiagKernel diag0, diag1;  // only for classes (X|X)
+    int bi, ki, L, nout;
+};
+
+}  // namespace hfgpu

@@ -1,0 +1,809 @@
+// B200 (sm_100a) direct-SCF Fock builder: device kernels and the C ABI.
+//
+// Replaces the reference's fock_build_initial_diag / fock_build_diag /
+// fock_build_non_diag (+ _j_only) subroutines (brichjnh/hfcode, Fortran +
+// OpenMP) with CUDA kernels that keep every piece of state resident in HBM:
+//
+//   k_maxdm        evaluate_maxdm.f90:1-101 -- max |P| per shell-pair block
+//                  (incl. the reference's d-l block choice, evaluate_maxdm.f90:82-89)
+//   k_diag<C,M>    fock_build_initial_diag.f90 (M=0: Schwarz factors, element
+//                  skip |e|>1e-10) and fock_build_diag.f90 (M=1: density
+//                  screen schw^2*max(D_ab,D_aa/4,D_bb/4) < thr)
+//   k_screen       the per-quartet screen of fock_build_non_diag.f90:63-67
+//                  (schw_ab*schw_cd*max(Dcoul,Dexch/4) < thr), evaluated for
+//                  every candidate pair of active shell pairs and compacted
+//                  into per-class quartet lists with warp ballots
+//   k_nondiag<C>   one thread per screened shell quartet: contracted (ab|cd)
+//                  from the generated class function, the post-screen
+//                  max|e| < thr (fock_build_non_diag.f90:69), then the J/K
+//                  scatter with FP64 atomics into a one-triangle buffer G
+//   k_symm         F += G + G^T (the reference writes both triangles)
+//
+// The reference's per-case scatter branches (aa|aa), (aa|bc), (ab|cd), ...
+// (fock_build_non_diag.f90:70-117 and 45 more blocks) all add the standard
+// RHF J - K/2 contribution of each unique AO quartet; here every ordered
+// component of a shell quartet carries the quartet's uniform degeneracy weight
+// s = (bra perms)(ket perms)(bra-ket perms)/8, which sums to the same F.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "../../include/hfgpu.h"
+#include "common.cuh"
+
+namespace hfgpu {
+#define HF_DECL_REG(ci) void register_class_##ci(ClassKernels* k);
+HF_DECL_REG(0) HF_DECL_REG(1) HF_DECL_REG(2) HF_DECL_REG(3) HF_DECL_REG(4) HF_DECL_REG(5) HF_DECL_REG(6)
+HF_DECL_REG(7) HF_DECL_REG(8) HF_DECL_REG(9) HF_DECL_REG(10) HF_DECL_REG(11) HF_DECL_REG(12) HF_DECL_REG(13)
+HF_DECL_REG(14) HF_DECL_REG(15) HF_DECL_REG(16) HF_DECL_REG(17) HF_DECL_REG(18) HF_DECL_REG(19) HF_DECL_REG(20)
+#undef HF_DECL_REG
+}  // namespace hfgpu
+
+using namespace hfgpu;
+
+namespace {
+
+thread_local std::string g_err;
+
+#define HF_CHECK(call)                                                                   \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) {                                                         \
+            g_err = std::string(#call) + ": " + cudaGetErrorString(e_);                  \
+            return HFGPU_ERR_CUDA;                                                       \
+        }                                                                                \
+    } while (0)
+
+constexpr double SHTHRESH = 1e-11;      // molprops.f90:163
+constexpr double EXTRATHRESH = 1e-12;   // precalc_kabs.f90:13
+
+// evaluate_maxdm.f90: one thread per unordered shell pair.
+__global__ void k_maxdm(const int* __restrict__ shtyp, const int* __restrict__ aosh, int nsh, int nb,
+                        const double* __restrict__ P, double* __restrict__ md) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long npair = (long long)nsh * (nsh + 1) / 2;
+    if (t >= npair) return;
+    int a = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while ((long long)a * (a + 1) / 2 > t) --a;
+    while ((long long)(a + 1) * (a + 2) / 2 <= t) ++a;
+    const int b = (int)(t - (long long)a * (a + 1) / 2);
+    auto rank = [](int ty) { return ty == 1 ? 0 : ty == 2 ? 1 : ty == 3 ? 2 : 3; };
+    auto nf = [](int ty) { return ty == 1 ? 1 : ty == 2 ? 3 : ty == 3 ? 5 : 4; };
+    int r = a, c = b;  // the reference's list orientation: lower rank first
+    if (rank(shtyp[r]) > rank(shtyp[c])) { int x = r; r = c; c = x; }
+    int nr = nf(shtyp[r]), nc = nf(shtyp[c]);
+    if (shtyp[r] == 3 && shtyp[c] == 12) { nr = 4; nc = 5; }  // evaluate_maxdm.f90:82-89
+    const int r0 = aosh[r], c0 = aosh[c];
+    double m = 0.0;
+    for (int i = 0; i < nr; ++i)
+        for (int j = 0; j < nc; ++j) {
+            const int row = r0 + i, col = c0 + j;
+            if (row < nb && col < nb) m = fmax(m, fabs(P[row + (size_t)col * nb]));
+        }
+    md[(size_t)a * nsh + b] = m;
+    md[(size_t)b * nsh + a] = m;
+}
+
+struct ScreenClass {
+    long long start;   // first padded candidate index of this class
+    long long ncand;   // candidates (unpadded)
+    long long cap;     // slots in the quartet list segment
+    long long qoff;    // offset of the segment
+    int same;          // bra type == ket type (triangular enumeration)
+    int nket;
+    const int2* bsh;   // (sa, sb) per active bra pair
+    const int2* ksh;
+    const double* bschw;
+    const double* kschw;
+};
+
+// Per-quartet screen of fock_build_non_diag.f90:63-67, compacted into the
+// class's list.  Candidates of each class are padded to a multiple of 32 so a
+// warp never spans two classes.
+__global__ void k_screen(const ScreenClass* __restrict__ cls, int ncls, long long ntot,
+                         const double* __restrict__ md, int nsh, double thr, int jonly, double f32cut,
+                         uint2* __restrict__ qbuf, unsigned long long* __restrict__ cnt) {
+    __shared__ ScreenClass sc[NCLS];
+    for (int i = threadIdx.x; i < ncls; i += blockDim.x) sc[i] = cls[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const long long nwarps_total = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long w = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); w * 32 < ntot;
+         w += nwarps_total) {
+        const long long t = w * 32 + lane;
+        const long long w0 = w * 32;
+        int c = 0;
+        while (c + 1 < ncls && sc[c + 1].start <= w0) ++c;
+        const ScreenClass& C = sc[c];
+        const long long u = t - C.start;
+        bool pass = false, lo = false;
+        unsigned ii = 0, jj = 0;
+        if (u < C.ncand) {
+            if (C.same) {
+                long long i = (long long)((1.0 + sqrt(1.0 + 8.0 * (double)u)) * 0.5);
+                while (i * (i - 1) / 2 > u) --i;
+                while ((i + 1) * i / 2 <= u) ++i;
+                ii = (unsigned)i;
+                jj = (unsigned)(u - i * (i - 1) / 2);
+            } else {
+                ii = (unsigned)(u / C.nket);
+                jj = (unsigned)(u - (long long)ii * C.nket);
+            }
+            const int2 ab = C.bsh[ii], cd = C.ksh[jj];
+            const double dc = fmax(md[ab.x * nsh + ab.y], md[cd.x * nsh + cd.y]);
+            double v = dc;
+            if (!jonly) {
+                const double dx = fmax(fmax(md[ab.x * nsh + cd.x], md[ab.x * nsh + cd.y]),
+                                       fmax(md[ab.y * nsh + cd.x], md[ab.y * nsh + cd.y]));
+                v = fmax(dc, 0.25 * dx);
+            }
+            const double bound = C.bschw[ii] * C.kschw[jj] * v;
+            pass = !(bound < thr);
+            lo = pass && bound < f32cut;
+        }
+        const unsigned m64 = __ballot_sync(0xffffffffu, pass && !lo);
+        const unsigned m32 = __ballot_sync(0xffffffffu, lo);
+        unsigned long long b64 = 0, b32 = 0;
+        if (lane == 0) {
+            if (m64) b64 = atomicAdd(&cnt[2 * c], (unsigned long long)__popc(m64));
+            if (m32) b32 = atomicAdd(&cnt[2 * c + 1], (unsigned long long)__popc(m32));
+        }
+        b64 = __shfl_sync(0xffffffffu, b64, 0);
+        b32 = __shfl_sync(0xffffffffu, b32, 0);
+        const unsigned lt = (1u << lane) - 1u;
+        if (pass && !lo) qbuf[C.qoff + (long long)b64 + __popc(m64 & lt)] = make_uint2(ii, jj);
+        if (lo) qbuf[C.qoff + C.cap - 1 - ((long long)b32 + __popc(m32 & lt))] = make_uint2(ii, jj);
+    }
+}
+
+// FMA-chain throughput probe: 8 independent chains per thread so the FP64 and
+// FP32 pipes, not latency, bound it.  Used to state the FP64/FP32 roofline.
+template <typename T>
+__global__ void k_fma_peak(T* out, int iters, T a, T b) {
+    T x[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) x[i] = (T)(threadIdx.x + i);
+    for (int it = 0; it < iters; ++it)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) x[i] = x[i] * a + b;
+    T s = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s += x[i];
+    if (s == (T)-1.2345) out[0] = s;  // keeps the chains live
+}
+
+__global__ void k_symm(double* __restrict__ F, const double* __restrict__ G, int nb) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)nb * nb) return;
+    const int i = (int)(t % nb), j = (int)(t / nb);
+    F[t] += G[t] + G[j + (size_t)i * nb];
+}
+
+// ------------------------------------------------------------- host ----
+struct HostPair {
+    GPair g;
+    int refcls;   // reference class index 0..9 (ss sp sd sl pp pd pl dd dl ll)
+    int refpos;   // position in the reference's class list
+};
+
+int ref_rank(int t) { return t == HFGPU_SHELL_S ? 0 : t == HFGPU_SHELL_P ? 1 : t == HFGPU_SHELL_D ? 2 : 3; }
+int nfunc_of(int t) { return t == HFGPU_SHELL_S ? 1 : t == HFGPU_SHELL_P ? 3 : t == HFGPU_SHELL_D ? 5 : 4; }
+
+// reference class (ss sp sd sl pp pd pl dd dl ll) of a rank pair (r1 <= r2)
+int ref_class(int r1, int r2) {
+    static const int tab[4][4] = {{0, 1, 2, 3}, {-1, 4, 5, 6}, {-1, -1, 7, 8}, {-1, -1, -1, 9}};
+    return tab[r1][r2];
+}
+// GPU pair type of a reference class, and whether the GPU pair swaps the
+// reference's (first, second) order; -1 for classes with pure p shells.
+int gpu_type_of_ref(int rc, bool* swap) {
+    switch (rc) {
+        case 0: *swap = false; return 0;  // ss -> SS
+        case 3: *swap = true; return 1;   // sl -> LS
+        case 9: *swap = false; return 2;  // ll -> LL
+        case 2: *swap = true; return 3;   // sd -> DS
+        case 8: *swap = false; return 4;  // dl -> DL
+        case 7: *swap = false; return 5;  // dd -> DD
+        default: *swap = false; return -1;
+    }
+}
+const int GPU_TO_REF[NPT] = {0, 3, 9, 2, 8, 7};
+
+long double boys_series(int m, long double T) {
+    // F_m(T) = e^-T sum_k (2T)^k / ((2m+1)(2m+3)...(2m+2k+1))
+    long double term = 1.0L / (2 * m + 1), sum = term;
+    for (int k = 1; k < 400; ++k) {
+        term *= 2.0L * T / (2 * m + 2 * k + 1);
+        sum += term;
+        if (term < sum * 1e-22L) break;
+    }
+    return expl(-T) * sum;
+}
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t n = 0;
+};
+
+}  // namespace
+
+struct hfgpu_handle {
+    int nsh = 0, nb = 0, npairs = 0;
+    std::vector<int> shtyp, nzet, aosh;
+    std::vector<HostPair> pairs[NPT];     // all pairs per GPU type
+    std::vector<int> refcount;            // pairs per reference class
+    std::vector<double> schw[NPT];        // host copy, by pair index
+    std::vector<int> last_ref;            // lastXX per reference class
+    bool have_schwarz = false;
+    int timing = 0;
+    cudaStream_t stream = nullptr;
+    // device
+    int* d_shtyp = nullptr;
+    int* d_aosh = nullptr;
+    GPrim* d_prims = nullptr;
+    GPair* d_pairs[NPT] = {};
+    double* d_schw[NPT] = {};
+    GPair* d_apairs[NPT] = {};
+    int2* d_ash[NPT] = {};
+    double* d_aschw[NPT] = {};
+    int nact[NPT] = {};
+    double* d_boys = nullptr;
+    float* d_boysf = nullptr;
+    double* d_P = nullptr;
+    double* d_F = nullptr;
+    double* d_G = nullptr;
+    double* d_md = nullptr;
+    ScreenClass* d_cls = nullptr;
+    uint2* d_q = nullptr;
+    size_t qcap = 0;
+    unsigned long long* d_cnt = nullptr;
+    ClassStats* d_stats = nullptr;
+    // last build statistics
+    long long st_pass[NCLS] = {}, st_scat[NCLS] = {}, st_prim[NCLS] = {}, st_f32[NCLS] = {};
+    double st_ms[NCLS] = {};
+    ScreenClass hcls[NCLS];
+    long long ntot = 0;
+    cudaEvent_t ev[2 * NCLS + 2] = {};
+};
+
+namespace {
+
+int set_err(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+template <typename T>
+int dalloc(T** p, size_t n) {
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        g_err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+        return HFGPU_ERR_NOMEM;
+    }
+    return HFGPU_OK;
+}
+
+// class index of pair types (i <= j), enumerated row by row
+int class_index(int i, int j) {
+    int c = 0;
+    for (int a = 0; a < NPT; ++a)
+        for (int b = a; b < NPT; ++b, ++c)
+            if (a == i && b == j) return c;
+    return -1;
+}
+
+struct ClassTable {
+    ClassKernels k[NCLS];
+    ClassTable() {
+        void (*reg[NCLS])(ClassKernels*) = {
+            register_class_0, register_class_1, register_class_2, register_class_3, register_class_4,
+            register_class_5, register_class_6, register_class_7, register_class_8, register_class_9,
+            register_class_10, register_class_11, register_class_12, register_class_13, register_class_14,
+            register_class_15, register_class_16, register_class_17, register_class_18, register_class_19,
+            register_class_20};
+        for (int c = 0; c < NCLS; ++c) reg[c](&k[c]);
+    }
+};
+const ClassTable& class_table() {
+    static ClassTable t;
+    return t;
+}
+#define CLASS_KERNELS (class_table().k)
+
+DiagKernel diag_kernel(int pt, int mode) {
+    const ClassKernels& k = CLASS_KERNELS[class_index(pt, pt)];
+    return mode ? k.diag1 : k.diag0;
+}
+
+int upload_fp(hfgpu_handle* h, const double* f, const double* p) {
+    size_t bytes = (size_t)h->nb * h->nb * sizeof(double);
+    HF_CHECK(cudaMemcpyAsync(h->d_P, p, bytes, cudaMemcpyHostToDevice, h->stream));
+    HF_CHECK(cudaMemcpyAsync(h->d_F, f, bytes, cudaMemcpyHostToDevice, h->stream));
+    return HFGPU_OK;
+}
+
+int download_f(hfgpu_handle* h, double* f) {
+    size_t bytes = (size_t)h->nb * h->nb * sizeof(double);
+    HF_CHECK(cudaMemcpyAsync(f, h->d_F, bytes, cudaMemcpyDeviceToHost, h->stream));
+    HF_CHECK(cudaStreamSynchronize(h->stream));
+    return HFGPU_OK;
+}
+
+int launch_maxdm(hfgpu_handle* h, const double* P) {
+    long long np = (long long)h->nsh * (h->nsh + 1) / 2;
+    int blocks = (int)((np + 255) / 256);
+    k_maxdm<<<blocks, 256, 0, h->stream>>>(h->d_shtyp, h->d_aosh, h->nsh, h->nb, P, h->d_md);
+    HF_CHECK(cudaGetLastError());
+    return HFGPU_OK;
+}
+
+int launch_symm(hfgpu_handle* h, double* F) {
+    long long n = (long long)h->nb * h->nb;
+    k_symm<<<(int)((n + 255) / 256), 256, 0, h->stream>>>(F, h->d_G, h->nb);
+    HF_CHECK(cudaGetLastError());
+    return HFGPU_OK;
+}
+
+int launch_diag(hfgpu_handle* h, int mode, const double* P, double thr) {
+    for (int t = 0; t < NPT; ++t) {
+        int n = (int)h->pairs[t].size();
+        if (n == 0) continue;
+        DiagArgs a{h->d_pairs[t], n, h->d_prims, h->d_boys, h->d_schw[t], h->d_md, h->nsh, P, h->d_G, h->nb, thr};
+        diag_kernel(t, mode)<<<(n + ND_THREADS - 1) / ND_THREADS, ND_THREADS, 0, h->stream>>>(a);
+        HF_CHECK(cudaGetLastError());
+    }
+    return HFGPU_OK;
+}
+
+// Schwarz ordering (index_sort + find_threshold) and the active pair arrays.
+int build_active(hfgpu_handle* h) {
+    for (int t = 0; t < NPT; ++t) {
+        int n = (int)h->pairs[t].size();
+        h->schw[t].resize(n);
+        if (n) HF_CHECK(cudaMemcpy(h->schw[t].data(), h->d_schw[t], n * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    h->last_ref.assign(10, 0);
+    long long total_q = 0;
+    for (int t = 0; t < NPT; ++t) {
+        const int n = (int)h->pairs[t].size();
+        // reference list order is refpos; pairs[t] is stored in that order
+        std::vector<int> ord(n);
+        std::iota(ord.begin(), ord.end(), 0);
+        std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return h->schw[t][x] > h->schw[t][y]; });
+        int last = 0;
+        if (n > 0) {
+            if (h->schw[t][ord[0]] < SHTHRESH) last = 1;
+            else if (h->schw[t][ord[n - 1]] > SHTHRESH) last = n;
+            else {
+                last = n;
+                for (int i = 0; i < n; ++i)
+                    if (h->schw[t][ord[i]] < SHTHRESH) { last = i + 1; break; }
+            }
+        }
+        h->last_ref[GPU_TO_REF[t]] = last;
+        // active set, re-ordered for the GPU: primitive count, then Schwarz
+        std::vector<int> act(ord.begin(), ord.begin() + last);
+        std::stable_sort(act.begin(), act.end(), [&](int x, int y) {
+            int nx = h->pairs[t][x].g.np, ny = h->pairs[t][y].g.np;
+            if (nx != ny) return nx > ny;
+            return h->schw[t][x] > h->schw[t][y];
+        });
+        std::vector<GPair> ap(last);
+        std::vector<int2> ash(last);
+        std::vector<double> asc(last);
+        for (int i = 0; i < last; ++i) {
+            ap[i] = h->pairs[t][act[i]].g;
+            ash[i] = make_int2(ap[i].sa, ap[i].sb);
+            asc[i] = h->schw[t][act[i]];
+        }
+        h->nact[t] = last;
+        if (last) {
+            HF_CHECK(cudaMemcpy(h->d_apairs[t], ap.data(), last * sizeof(GPair), cudaMemcpyHostToDevice));
+            HF_CHECK(cudaMemcpy(h->d_ash[t], ash.data(), last * sizeof(int2), cudaMemcpyHostToDevice));
+            HF_CHECK(cudaMemcpy(h->d_aschw[t], asc.data(), last * sizeof(double), cudaMemcpyHostToDevice));
+        }
+    }
+    // screening descriptors and quartet-list segments
+    long long start = 0, qoff = 0;
+    for (int c = 0; c < NCLS; ++c) {
+        const int bi = CLASS_KERNELS[c].bi, ki = CLASS_KERNELS[c].ki;
+        ScreenClass& s = h->hcls[c];
+        const long long nb_ = h->nact[bi], nk = h->nact[ki];
+        s.same = bi == ki;
+        s.ncand = s.same ? nb_ * (nb_ - 1) / 2 : nb_ * nk;
+        s.nket = (int)nk;
+        s.start = start;
+        s.cap = s.ncand;
+        s.qoff = qoff;
+        s.bsh = h->d_ash[bi];
+        s.ksh = h->d_ash[ki];
+        s.bschw = h->d_aschw[bi];
+        s.kschw = h->d_aschw[ki];
+        start += (s.ncand + 31) / 32 * 32;
+        qoff += s.cap;
+    }
+    h->ntot = start;
+    total_q = qoff;
+    HF_CHECK(cudaMemcpy(h->d_cls, h->hcls, sizeof(h->hcls), cudaMemcpyHostToDevice));
+    if ((size_t)total_q > h->qcap) {
+        if (h->d_q) cudaFree(h->d_q);
+        h->d_q = nullptr;
+        h->qcap = 0;
+        int rc = dalloc(&h->d_q, (size_t)total_q);
+        if (rc) return rc;
+        h->qcap = (size_t)std::max<long long>(total_q, 1);
+    }
+    h->have_schwarz = true;
+    return HFGPU_OK;
+}
+
+int run_non_diag(hfgpu_handle* h, const double* P, double thr, int jonly, double f32cut) {
+    if (!h->have_schwarz) return set_err(HFGPU_ERR_STATE, "fock_build_initial_diag has not been called");
+    HF_CHECK(cudaMemsetAsync(h->d_cnt, 0, 2 * NCLS * sizeof(unsigned long long), h->stream));
+    HF_CHECK(cudaMemsetAsync(h->d_stats, 0, NCLS * sizeof(ClassStats), h->stream));
+    if (h->ntot > 0) {
+        int dev = 0, nsm = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        long long warps = h->ntot / 32;
+        long long blocks = std::min<long long>((warps + 7) / 8, (long long)nsm * 64);
+        k_screen<<<(int)blocks, 256, 0, h->stream>>>(h->d_cls, NCLS, h->ntot, h->d_md, h->nsh, thr, jonly, f32cut,
+                                                      h->d_q, h->d_cnt);
+        HF_CHECK(cudaGetLastError());
+    }
+    unsigned long long cnt[2 * NCLS];
+    HF_CHECK(cudaMemcpyAsync(cnt, h->d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, h->stream));
+    HF_CHECK(cudaStreamSynchronize(h->stream));
+    for (int c = 0; c < NCLS; ++c) {
+        const ClassKernels& K = CLASS_KERNELS[c];
+        h->st_pass[c] = (long long)(cnt[2 * c] + cnt[2 * c + 1]);
+        h->st_ms[c] = 0.0;
+        for (int prec = 0; prec < 2; ++prec) {
+            long long n = (long long)cnt[2 * c + prec];
+            if (n == 0) continue;
+            NDArgs a{h->d_q + h->hcls[c].qoff, (int)n, prec, h->hcls[c].cap, h->d_apairs[K.bi], h->d_apairs[K.ki],
+                     h->d_prims, h->d_boys, h->d_boysf, P, h->d_G, h->nb, thr, jonly, h->d_stats + c};
+            long long blocks = (n + ND_THREADS - 1) / ND_THREADS;
+            if (h->timing) HF_CHECK(cudaEventRecord(h->ev[2 * c], h->stream));
+            (prec ? K.nd32 : K.nd64)<<<(int)blocks, ND_THREADS, 0, h->stream>>>(a);
+            HF_CHECK(cudaGetLastError());
+            if (h->timing) {
+                HF_CHECK(cudaEventRecord(h->ev[2 * c + 1], h->stream));
+                HF_CHECK(cudaEventSynchronize(h->ev[2 * c + 1]));
+                float ms = 0;
+                cudaEventElapsedTime(&ms, h->ev[2 * c], h->ev[2 * c + 1]);
+                h->st_ms[c] += ms;
+            }
+        }
+    }
+    ClassStats st[NCLS];
+    HF_CHECK(cudaMemcpyAsync(st, h->d_stats, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+    HF_CHECK(cudaStreamSynchronize(h->stream));
+    for (int c = 0; c < NCLS; ++c) {
+        h->st_scat[c] = (long long)st[c].scattered;
+        h->st_prim[c] = (long long)st[c].prim;
+        h->st_f32[c] = (long long)st[c].fp32;
+    }
+    return HFGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* hfgpu_last_error(void) { return g_err.c_str(); }
+
+int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
+    if (!B || !out || B->nsh <= 0 || B->nb <= 0 || B->maxprim <= 0)
+        return set_err(HFGPU_ERR_ARG, "hfgpu_init: bad arguments");
+    *out = nullptr;
+    hfgpu_handle* h = new hfgpu_handle();
+    h->nsh = B->nsh;
+    h->nb = B->nb;
+    h->shtyp.assign(B->shtyp, B->shtyp + B->nsh);
+    h->nzet.assign(B->nzet, B->nzet + B->nsh);
+    h->aosh.assign(B->aosh, B->aosh + B->nsh);
+    const int MP = B->maxprim;
+    const double PI = 3.141592653589793238462643383279502884197;
+    const double RT2PI54 = std::sqrt(2.0 * PI * PI * std::sqrt(PI));
+    for (int s = 0; s < h->nsh; ++s) {
+        int t = h->shtyp[s];
+        if (t != HFGPU_SHELL_S && t != HFGPU_SHELL_D && t != HFGPU_SHELL_L) {
+            delete h;
+            return set_err(HFGPU_ERR_UNSUPPORTED, "hfgpu_init: pure p shells are not supported by the GPU classes");
+        }
+        if (h->nzet[s] < 1 || h->nzet[s] > MP) {
+            delete h;
+            return set_err(HFGPU_ERR_ARG, "hfgpu_init: bad primitive count");
+        }
+    }
+    // pair lists in the reference's enumeration order (precalc_kabs.f90:38-90)
+    std::vector<GPrim> prims;
+    h->refcount.assign(10, 0);
+    for (int s1 = 0; s1 < h->nsh; ++s1)
+        for (int s2 = 0; s2 <= s1; ++s2) {
+            int r1 = s1, r2 = s2;
+            if (ref_rank(h->shtyp[r1]) > ref_rank(h->shtyp[r2])) std::swap(r1, r2);
+            int rc = ref_class(ref_rank(h->shtyp[r1]), ref_rank(h->shtyp[r2]));
+            bool swp = false;
+            int gt = gpu_type_of_ref(rc, &swp);
+            int a = swp ? r2 : r1, b = swp ? r1 : r2;
+            HostPair hp;
+            hp.refcls = rc;
+            hp.refpos = h->refcount[rc]++;
+            GPair& g = hp.g;
+            for (int x = 0; x < 3; ++x) {
+                g.A[x] = B->xsh[3 * a + x];
+                g.B[x] = B->xsh[3 * b + x];
+            }
+            g.sa = a;
+            g.sb = b;
+            g.aoa = B->aosh[a];
+            g.aob = B->aosh[b];
+            g.p0 = (int)prims.size();
+            double r2ab = 0;
+            for (int x = 0; x < 3; ++x) r2ab += (g.A[x] - g.B[x]) * (g.A[x] - g.B[x]);
+            for (int za = 0; za < h->nzet[a]; ++za)
+                for (int zb = 0; zb < h->nzet[b]; ++zb) {
+                    double ea = B->zeta[(size_t)a * MP + za], eb = B->zeta[(size_t)b * MP + zb];
+                    double p = ea + eb, pm1 = 1.0 / p, q = ea * eb * pm1;
+                    double K = RT2PI54 * std::exp(-q * r2ab) * pm1 * B->djk[(size_t)a * MP + za] *
+                               B->djk[(size_t)b * MP + zb];
+                    if (std::fabs(K) * std::sqrt(pm1) < EXTRATHRESH) continue;  // negab
+                    GPrim gp;
+                    gp.p = p;
+                    for (int x = 0; x < 3; ++x) gp.P[x] = (ea * g.A[x] + eb * g.B[x]) * pm1;
+                    gp.K = K;
+                    gp.w1 = h->shtyp[a] == HFGPU_SHELL_L ? B->djkl[(size_t)a * MP + za] : 1.0;
+                    gp.w2 = h->shtyp[b] == HFGPU_SHELL_L ? B->djkl[(size_t)b * MP + zb] : 1.0;
+                    gp.pad = 0.0;
+                    prims.push_back(gp);
+                }
+            g.np = (int)prims.size() - g.p0;
+            h->pairs[gt].push_back(hp);
+            h->npairs++;
+        }
+    // Boys tables: c_k = F_{M+k}(T_j) (-1)^k / k!, M = 0..8, T_j = j/8
+    std::vector<double> bt((size_t)(BOYS_MMAX + 1) * BOYS_NPT * BOYS_K);
+    std::vector<float> btf(bt.size());
+    for (int M = 0; M <= BOYS_MMAX; ++M)
+        for (int j = 0; j < BOYS_NPT; ++j) {
+            long double T = j / 8.0L, fact = 1.0L;
+            for (int k = 0; k < BOYS_K; ++k) {
+                if (k) fact *= k;
+                long double v = boys_series(M + k, T) / fact * ((k & 1) ? -1.0L : 1.0L);
+                size_t i = ((size_t)M * BOYS_NPT + j) * BOYS_K + k;
+                bt[i] = (double)v;
+                btf[i] = (float)v;
+            }
+        }
+    cudaError_t ce = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (ce != cudaSuccess) {
+        std::string m = std::string("cudaStreamCreate: ") + cudaGetErrorString(ce);
+        delete h;
+        return set_err(HFGPU_ERR_CUDA, m);
+    }
+    int rc = 0;
+    const size_t nb2 = (size_t)h->nb * h->nb;
+    rc |= dalloc(&h->d_shtyp, h->nsh);
+    rc |= dalloc(&h->d_aosh, h->nsh);
+    rc |= dalloc(&h->d_prims, prims.size());
+    rc |= dalloc(&h->d_boys, bt.size());
+    rc |= dalloc(&h->d_boysf, btf.size());
+    rc |= dalloc(&h->d_P, nb2);
+    rc |= dalloc(&h->d_F, nb2);
+    rc |= dalloc(&h->d_G, nb2);
+    rc |= dalloc(&h->d_md, (size_t)h->nsh * h->nsh);
+    rc |= dalloc(&h->d_cls, NCLS);
+    rc |= dalloc(&h->d_cnt, 2 * NCLS);
+    rc |= dalloc(&h->d_stats, NCLS);
+    for (int t = 0; t < NPT; ++t) {
+        size_t n = h->pairs[t].size();
+        rc |= dalloc(&h->d_pairs[t], n);
+        rc |= dalloc(&h->d_schw[t], n);
+        rc |= dalloc(&h->d_apairs[t], n);
+        rc |= dalloc(&h->d_ash[t], n);
+        rc |= dalloc(&h->d_aschw[t], n);
+    }
+    if (rc) {
+        hfgpu_finalize(h);
+        return HFGPU_ERR_NOMEM;
+    }
+    for (int i = 0; i < 2 * NCLS + 2; ++i) cudaEventCreate(&h->ev[i]);
+    auto up = [&](void* d, const void* s, size_t bytes) {
+        if (bytes == 0) return cudaSuccess;
+        return cudaMemcpy(d, s, bytes, cudaMemcpyHostToDevice);
+    };
+    ce = up(h->d_shtyp, h->shtyp.data(), h->nsh * sizeof(int));
+    if (ce == cudaSuccess) ce = up(h->d_aosh, h->aosh.data(), h->nsh * sizeof(int));
+    if (ce == cudaSuccess) ce = up(h->d_prims, prims.data(), prims.size() * sizeof(GPrim));
+    if (ce == cudaSuccess) ce = up(h->d_boys, bt.data(), bt.size() * sizeof(double));
+    if (ce == cudaSuccess) ce = up(h->d_boysf, btf.data(), btf.size() * sizeof(float));
+    for (int t = 0; t < NPT && ce == cudaSuccess; ++t) {
+        std::vector<GPair> gp(h->pairs[t].size());
+        for (size_t i = 0; i < gp.size(); ++i) gp[i] = h->pairs[t][i].g;
+        ce = up(h->d_pairs[t], gp.data(), gp.size() * sizeof(GPair));
+    }
+    if (ce != cudaSuccess) {
+        std::string m = std::string("hfgpu_init upload: ") + cudaGetErrorString(ce);
+        hfgpu_finalize(h);
+        return set_err(HFGPU_ERR_CUDA, m);
+    }
+    *out = h;
+    return HFGPU_OK;
+}
+
+int hfgpu_finalize(hfgpu_handle* h) {
+    if (!h) return HFGPU_OK;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    void* bufs[] = {h->d_shtyp, h->d_aosh, h->d_prims, h->d_boys, h->d_boysf, h->d_P, h->d_F, h->d_G,
+                    h->d_md, h->d_cls, h->d_q, h->d_cnt, h->d_stats};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    for (int t = 0; t < NPT; ++t) {
+        void* tb[] = {h->d_pairs[t], h->d_schw[t], h->d_apairs[t], h->d_ash[t], h->d_aschw[t]};
+        for (void* b : tb)
+            if (b) cudaFree(b);
+    }
+    for (int i = 0; i < 2 * NCLS + 2; ++i)
+        if (h->ev[i]) cudaEventDestroy(h->ev[i]);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return HFGPU_OK;
+}
+
+int hfgpu_fock_build_initial_diag(hfgpu_handle* h, double* f, const double* p, double thr) {
+    if (!h || !f || !p) return set_err(HFGPU_ERR_ARG, "null argument");
+    int rc = upload_fp(h, f, p);
+    if (rc) return rc;
+    HF_CHECK(cudaMemsetAsync(h->d_G, 0, (size_t)h->nb * h->nb * sizeof(double), h->stream));
+    rc = launch_diag(h, 0, h->d_P, thr);
+    if (rc) return rc;
+    rc = launch_symm(h, h->d_F);
+    if (rc) return rc;
+    rc = download_f(h, f);
+    if (rc) return rc;
+    return build_active(h);
+}
+
+int hfgpu_fock_build_diag(hfgpu_handle* h, double* f, const double* p, double thr) {
+    if (!h || !f || !p) return set_err(HFGPU_ERR_ARG, "null argument");
+    if (!h->have_schwarz) return set_err(HFGPU_ERR_STATE, "fock_build_initial_diag has not been called");
+    int rc = upload_fp(h, f, p);
+    if (rc) return rc;
+    HF_CHECK(cudaMemsetAsync(h->d_G, 0, (size_t)h->nb * h->nb * sizeof(double), h->stream));
+    if ((rc = launch_maxdm(h, h->d_P))) return rc;
+    if ((rc = launch_diag(h, 1, h->d_P, thr))) return rc;
+    if ((rc = launch_symm(h, h->d_F))) return rc;
+    return download_f(h, f);
+}
+
+static int non_diag_host(hfgpu_handle* h, double* f, const double* p, double thr, int jonly, double f32cut) {
+    if (!h || !f || !p) return set_err(HFGPU_ERR_ARG, "null argument");
+    if (!h->have_schwarz) return set_err(HFGPU_ERR_STATE, "fock_build_initial_diag has not been called");
+    int rc = upload_fp(h, f, p);
+    if (rc) return rc;
+    HF_CHECK(cudaMemsetAsync(h->d_G, 0, (size_t)h->nb * h->nb * sizeof(double), h->stream));
+    if ((rc = launch_maxdm(h, h->d_P))) return rc;
+    if ((rc = run_non_diag(h, h->d_P, thr, jonly, f32cut))) return rc;
+    if ((rc = launch_symm(h, h->d_F))) return rc;
+    return download_f(h, f);
+}
+
+int hfgpu_fock_build_non_diag(hfgpu_handle* h, double* f, const double* p, double thr) {
+    return non_diag_host(h, f, p, thr, 0, 0.0);
+}
+
+int hfgpu_fock_build_non_diag_j_only(hfgpu_handle* h, double* f, const double* p, double thr) {
+    return non_diag_host(h, f, p, thr, 1, 0.0);
+}
+
+int hfgpu_fock_build_non_diag_mixed(hfgpu_handle* h, double* f, const double* p, double thr, double fp32_cutoff) {
+    return non_diag_host(h, f, p, thr, 0, fp32_cutoff);
+}
+
+int hfgpu_fock_build_device(hfgpu_handle* h, double* f_dev, const double* p_dev, double thr_diag,
+                            double thr_non_diag, double fp32_cutoff) {
+    if (!h || !f_dev || !p_dev) return set_err(HFGPU_ERR_ARG, "null argument");
+    if (!h->have_schwarz) return set_err(HFGPU_ERR_STATE, "fock_build_initial_diag has not been called");
+    int rc;
+    HF_CHECK(cudaMemsetAsync(h->d_G, 0, (size_t)h->nb * h->nb * sizeof(double), h->stream));
+    if ((rc = launch_maxdm(h, p_dev))) return rc;
+    if ((rc = launch_diag(h, 1, p_dev, thr_diag))) return rc;
+    if ((rc = run_non_diag(h, p_dev, thr_non_diag, 0, fp32_cutoff))) return rc;
+    return launch_symm(h, f_dev);
+}
+
+int hfgpu_dims(const hfgpu_handle* h, int* nb, int* nsh, int* npairs) {
+    if (!h) return set_err(HFGPU_ERR_ARG, "null handle");
+    if (nb) *nb = h->nb;
+    if (nsh) *nsh = h->nsh;
+    if (npairs) *npairs = h->npairs;
+    return HFGPU_OK;
+}
+
+int hfgpu_get_schwarz(const hfgpu_handle* h, double* schw_sh, int* last) {
+    if (!h) return set_err(HFGPU_ERR_ARG, "null handle");
+    if (!h->have_schwarz) return set_err(HFGPU_ERR_STATE, "fock_build_initial_diag has not been called");
+    if (schw_sh) {
+        for (int t = 0; t < NPT; ++t)
+            for (size_t i = 0; i < h->pairs[t].size(); ++i) {
+                const GPair& g = h->pairs[t][i].g;
+                schw_sh[(size_t)g.sa * h->nsh + g.sb] = h->schw[t][i];
+                schw_sh[(size_t)g.sb * h->nsh + g.sa] = h->schw[t][i];
+            }
+    }
+    if (last)
+        for (int c = 0; c < 10; ++c) last[c] = h->last_ref[c];
+    return HFGPU_OK;
+}
+
+int hfgpu_get_class_stats(const hfgpu_handle* h, long long* n_pass, long long* n_scattered, long long* n_prim,
+                          long long* n_fp32, double* ms) {
+    if (!h) return set_err(HFGPU_ERR_ARG, "null handle");
+    for (int c = 0; c < NCLS; ++c) {
+        if (n_pass) n_pass[c] = h->st_pass[c];
+        if (n_scattered) n_scattered[c] = h->st_scat[c];
+        if (n_prim) n_prim[c] = h->st_prim[c];
+        if (n_fp32) n_fp32[c] = h->st_f32[c];
+        if (ms) ms[c] = h->st_ms[c];
+    }
+    return HFGPU_OK;
+}
+
+int hfgpu_set_timing(hfgpu_handle* h, int on) {
+    if (!h) return set_err(HFGPU_ERR_ARG, "null handle");
+    h->timing = on;
+    return HFGPU_OK;
+}
+
+void* hfgpu_stream(hfgpu_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+int hfgpu_measure_fma_peak(double* fp64_gflops, double* fp32_gflops) {
+    int dev = 0, nsm = 0;
+    HF_CHECK(cudaGetDevice(&dev));
+    HF_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    double* dd = nullptr;
+    HF_CHECK(cudaMalloc(&dd, 64));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int threads = 256, blocks = nsm * 8, iters = 1 << 14;
+    double res[2] = {0, 0};
+    for (int prec = 0; prec < 2; ++prec) {
+        float best = 1e30f;
+        for (int rep = 0; rep < 4; ++rep) {
+            cudaEventRecord(e0);
+            if (prec == 0) k_fma_peak<double><<<blocks, threads>>>(dd, iters, 0.999999, 1e-7);
+            else k_fma_peak<float><<<blocks, threads>>>((float*)dd, iters, 0.999999f, 1e-7f);
+            cudaEventRecord(e1);
+            cudaError_t ce = cudaEventSynchronize(e1);
+            if (ce != cudaSuccess) {
+                cudaFree(dd);
+                g_err = cudaGetErrorString(ce);
+                return HFGPU_ERR_CUDA;
+            }
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep > 0) best = std::min(best, ms);
+        }
+        res[prec] = 2.0 * 8.0 * (double)iters * threads * blocks / (best * 1e-3) / 1e9;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(dd);
+    if (fp64_gflops) *fp64_gflops = res[0];
+    if (fp32_gflops) *fp32_gflops = res[1];
+    return HFGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,175 @@
+"""Python binding of the B200 Fock builder's C ABI (include/hfgpu.h).
+
+Mirrors the reference's Fock-builder interface: the same three entry points
+with the same arguments and the same accumulate semantics (f += G(p)), as
+called by direct_hartreefock.f90:101-121:
+
+    fb = FockBuilder(shells)
+    fb.fock_build_initial_diag(f, p, thr)   # cycle 1: Schwarz + diagonal pairs
+    fb.fock_build_non_diag(f, p, thr)
+    fb.fock_build_diag(f, p, thr)           # later cycles
+    fb.fock_build_non_diag(f, p, thr)
+
+There is no CPU fallback: importing this module fails if the CUDA library
+has not been built, and every call raises if the GPU reports an error.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Dict, Optional
+
+import numpy as np
+
+from .basis import ShellSet
+from .cabi import BasisDescriptor
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(_HERE, "libhfgpu.so")
+
+CLASS_NAMES = [f"{a}|{b}" for i, a in enumerate(["SS", "LS", "LL", "DS", "DL", "DD"])
+               for b in ["SS", "LS", "LL", "DS", "DL", "DD"][i:]]
+REF_CLASSES = ["ss", "sp", "sd", "sl", "pp", "pd", "pl", "dd", "dl", "ll"]
+
+
+class HfgpuError(RuntimeError):
+    pass
+
+
+def _load():
+    if not os.path.exists(LIBPATH):
+        raise ImportError(f"hfcode_b200: CUDA library {LIBPATH} is missing; run __graft_entry__.build()")
+    lib = ctypes.CDLL(LIBPATH)
+    d = ctypes.POINTER(ctypes.c_double)
+    i = ctypes.POINTER(ctypes.c_int)
+    ll = ctypes.POINTER(ctypes.c_longlong)
+    vp = ctypes.c_void_p
+    lib.hfgpu_init.argtypes = [vp, ctypes.POINTER(vp)]
+    for n in ("hfgpu_fock_build_initial_diag", "hfgpu_fock_build_diag", "hfgpu_fock_build_non_diag",
+              "hfgpu_fock_build_non_diag_j_only"):
+        getattr(lib, n).argtypes = [vp, d, d, ctypes.c_double]
+    lib.hfgpu_fock_build_non_diag_mixed.argtypes = [vp, d, d, ctypes.c_double, ctypes.c_double]
+    lib.hfgpu_fock_build_device.argtypes = [vp, vp, vp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+    lib.hfgpu_dims.argtypes = [vp, i, i, i]
+    lib.hfgpu_get_schwarz.argtypes = [vp, d, i]
+    lib.hfgpu_get_class_stats.argtypes = [vp, ll, ll, ll, ll, d]
+    lib.hfgpu_set_timing.argtypes = [vp, ctypes.c_int]
+    lib.hfgpu_stream.argtypes = [vp]
+    lib.hfgpu_stream.restype = vp
+    lib.hfgpu_finalize.argtypes = [vp]
+    lib.hfgpu_last_error.restype = ctypes.c_char_p
+    lib.hfgpu_measure_fma_peak.argtypes = [d, d]
+    return lib
+
+
+_lib = _load()
+
+EXPORTS = ["hfgpu_init", "hfgpu_fock_build_initial_diag", "hfgpu_fock_build_diag",
+           "hfgpu_fock_build_non_diag", "hfgpu_fock_build_non_diag_j_only",
+           "hfgpu_fock_build_non_diag_mixed", "hfgpu_fock_build_device", "hfgpu_dims",
+           "hfgpu_get_schwarz", "hfgpu_get_class_stats", "hfgpu_set_timing", "hfgpu_stream",
+           "hfgpu_finalize", "hfgpu_last_error", "hfgpu_measure_fma_peak"]
+
+
+def measure_fma_peak():
+    """(FP64, FP32) FMA throughput of the current GPU in GFLOP/s."""
+    a, b = ctypes.c_double(), ctypes.c_double()
+    _check(_lib.hfgpu_measure_fma_peak(ctypes.byref(a), ctypes.byref(b)), "measure_fma_peak")
+    return a.value, b.value
+
+
+def lib():
+    return _lib
+
+
+def _check(rc: int, what: str):
+    if rc != 0:
+        msg = _lib.hfgpu_last_error().decode(errors="replace")
+        raise HfgpuError(f"{what} failed (status {rc}): {msg}")
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class FockBuilder:
+    """One SCF instance's resident Fock-build state on the current GPU."""
+
+    def __init__(self, shells: ShellSet):
+        self.shells = shells
+        self.nb = shells.nb
+        self.nsh = shells.nsh
+        self._desc = BasisDescriptor(shells)
+        h = ctypes.c_void_p()
+        _check(_lib.hfgpu_init(ctypes.addressof(self._desc.struct), ctypes.byref(h)), "hfgpu_init")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.hfgpu_finalize(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _fp(self, f, p):
+        if f.shape != (self.nb, self.nb) or p.shape != (self.nb, self.nb):
+            raise ValueError("f and p must be nb x nb")
+        if f.dtype != np.float64 or not (f.flags["C_CONTIGUOUS"] or f.flags["F_CONTIGUOUS"]):
+            raise ValueError("f must be a contiguous float64 array (updated in place)")
+        pp = np.ascontiguousarray(p, dtype=np.float64)
+        return _dp(f), _dp(pp), pp
+
+    # --- the reference's entry points -------------------------------------
+    def fock_build_initial_diag(self, f: np.ndarray, p: np.ndarray, thr: float):
+        fp, pp, keep = self._fp(f, p)
+        _check(_lib.hfgpu_fock_build_initial_diag(self.h, fp, pp, float(thr)), "fock_build_initial_diag")
+
+    def fock_build_diag(self, f: np.ndarray, p: np.ndarray, thr: float):
+        fp, pp, keep = self._fp(f, p)
+        _check(_lib.hfgpu_fock_build_diag(self.h, fp, pp, float(thr)), "fock_build_diag")
+
+    def fock_build_non_diag(self, f: np.ndarray, p: np.ndarray, thr: float):
+        fp, pp, keep = self._fp(f, p)
+        _check(_lib.hfgpu_fock_build_non_diag(self.h, fp, pp, float(thr)), "fock_build_non_diag")
+
+    def fock_build_non_diag_j_only(self, f: np.ndarray, p: np.ndarray, thr: float):
+        fp, pp, keep = self._fp(f, p)
+        _check(_lib.hfgpu_fock_build_non_diag_j_only(self.h, fp, pp, float(thr)), "fock_build_non_diag_j_only")
+
+    # --- additions --------------------------------------------------------
+    def fock_build_non_diag_mixed(self, f: np.ndarray, p: np.ndarray, thr: float, fp32_cutoff: float):
+        fp, pp, keep = self._fp(f, p)
+        _check(_lib.hfgpu_fock_build_non_diag_mixed(self.h, fp, pp, float(thr), float(fp32_cutoff)),
+               "fock_build_non_diag_mixed")
+
+    def fock_build_device(self, f_ptr: int, p_ptr: int, thr_diag: float, thr_non_diag: float,
+                          fp32_cutoff: float = 0.0):
+        """Full build on device pointers (e.g. torch tensors' data_ptr())."""
+        _check(_lib.hfgpu_fock_build_device(self.h, ctypes.c_void_p(f_ptr), ctypes.c_void_p(p_ptr),
+                                            float(thr_diag), float(thr_non_diag), float(fp32_cutoff)),
+               "fock_build_device")
+
+    def stream(self) -> int:
+        return int(_lib.hfgpu_stream(self.h) or 0)
+
+    def set_timing(self, on: bool):
+        _check(_lib.hfgpu_set_timing(self.h, 1 if on else 0), "set_timing")
+
+    def schwarz(self):
+        s = np.zeros((self.nsh, self.nsh))
+        last = (ctypes.c_int * 10)()
+        _check(_lib.hfgpu_get_schwarz(self.h, _dp(s), last), "get_schwarz")
+        return s, dict(zip(REF_CLASSES, list(last)))
+
+    def class_stats(self) -> Dict[str, np.ndarray]:
+        arrs = [(ctypes.c_longlong * 21)() for _ in range(4)]
+        ms = (ctypes.c_double * 21)()
+        _check(_lib.hfgpu_get_class_stats(self.h, *arrs, ms), "get_class_stats")
+        keys = ["pass", "scattered", "prim", "fp32"]
+        out = {k: np.array(list(a), dtype=np.int64) for k, a in zip(keys, arrs)}
+        out["ms"] = np.array(list(ms))
+        return out

@@ -1,0 +1,128 @@
+/*
+ * hfgpu.h -- C ABI of the B200 direct-SCF Fock builder.
+ *
+ * Drop-in boundary for the reference's Fock builders.  Each entry point
+ * replaces one external subroutine of brichjnh/hfcode that
+ * direct_hartreefock.f90 calls (direct_hartreefock.f90:101-121); the
+ * Fortran side binds them through iso_c_binding.
+ *
+ * Conventions shared by all entry points
+ *   - f and p are caller-owned HOST arrays of nb x nb doubles, column-major
+ *     (Fortran layout); p must be symmetric.
+ *   - Semantics are accumulate: f += G(p), both triangles written, as the
+ *     reference does (F = H + J - K/2 with the total density p = 2 C C^T).
+ *   - Return 0 on success, non-zero on error; hfgpu_last_error() describes
+ *     the last error of the calling thread.  The reference has no error
+ *     convention (its subroutines `stop`); a Fortran shim `error stop`s on a
+ *     non-zero return.
+ *   - Calls on one handle are serialised on the handle's CUDA stream and are
+ *     synchronous with respect to the host buffers they receive.  Different
+ *     handles are independent.
+ */
+#ifndef HFGPU_H
+#define HFGPU_H
+
+#include "hfgpu_basis.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct hfgpu_handle hfgpu_handle;
+
+/* Status codes. */
+#define HFGPU_OK 0
+#define HFGPU_ERR_ARG 1
+#define HFGPU_ERR_CUDA 2
+#define HFGPU_ERR_STATE 3
+#define HFGPU_ERR_UNSUPPORTED 4
+#define HFGPU_ERR_NOMEM 5
+
+/* Replaces the one-time set-up the reference runs after reading the basis:
+ * precalcs_kabs (precalc_kabs.f90:1-296: pair lists, primitive-pair data,
+ * negab screen) and the Boys tables (index_functions.f90:171-226).
+ * Uploads the shell data to the current CUDA device. */
+int hfgpu_init(const hfgpu_basis* basis, hfgpu_handle** out);
+
+/* Replaces fock_build_initial_diag(f,p,thr) (fock_build_initial_diag.f90:1-818):
+ * (ab|ab) integrals of every shell pair, their Fock contributions with the
+ * |e| > 1e-10 element skip, the Schwarz factors and their sorted, truncated
+ * order (the reference's schwXX/orderXX/lastXX side effects,
+ * fock_build_initial_diag.f90:51-52 ... 810-811).  Must precede the calls
+ * below. */
+int hfgpu_fock_build_initial_diag(hfgpu_handle* h, double* f, const double* p, double thr);
+
+/* Replaces fock_build_diag(f,p,thr) (fock_build_diag.f90:1-692). */
+int hfgpu_fock_build_diag(hfgpu_handle* h, double* f, const double* p, double thr);
+
+/* Replaces fock_build_non_diag(f,p,thr) (fock_build_non_diag.f90:1-3412;
+ * fock_build_non_diag_k.f90 is an identical copy). */
+int hfgpu_fock_build_non_diag(hfgpu_handle* h, double* f, const double* p, double thr);
+
+/* Replaces fock_build_non_diag_j_only(f,p,thr) (fock_build_non_diag_j.f90:1-2354):
+ * Coulomb part only, screened by schw_ab*schw_cd*max(D_ab,D_cd). */
+int hfgpu_fock_build_non_diag_j_only(hfgpu_handle* h, double* f, const double* p, double thr);
+
+/* Mixed-precision off-diagonal build (no reference counterpart; the
+ * reference is FP64 only, nrtype.f90:8-9).  Shell quartets whose screening
+ * bound schw_ab*schw_cd*max(Dcoul,Dexch/4) falls below fp32_cutoff are
+ * evaluated in FP32 (FP32 Boys, recurrences and contraction), the rest in
+ * FP64; accumulation into f is FP64.  fp32_cutoff = 0 gives the FP64 build. */
+int hfgpu_fock_build_non_diag_mixed(hfgpu_handle* h, double* f, const double* p, double thr,
+                                    double fp32_cutoff);
+
+/* Device-resident variant for callers that keep F and P in HBM: one full
+ * build (fock_build_diag with thr_diag + fock_build_non_diag with
+ * thr_non_diag, optionally mixed) on device pointers, enqueued on the
+ * handle's stream without host synchronisation except for reading the
+ * per-class quartet counts.  f_dev += G(p_dev). */
+int hfgpu_fock_build_device(hfgpu_handle* h, double* f_dev, const double* p_dev, double thr_diag,
+                            double thr_non_diag, double fp32_cutoff);
+
+/* Number of basis functions / shells / shell pairs of the handle. */
+int hfgpu_dims(const hfgpu_handle* h, int* nb, int* nsh, int* npairs);
+
+/* Schwarz state left by hfgpu_fock_build_initial_diag: schw_sh (nsh x nsh,
+ * row-major, symmetric) = sqrt(max |(ab|ab)|) per shell pair; last[10] =
+ * the reference's lastXX per pair class in the order
+ * ss, sp, sd, sl, pp, pd, pl, dd, dl, ll (index_sort.f90:95-119). */
+int hfgpu_get_schwarz(const hfgpu_handle* h, double* schw_sh, int* last);
+
+/* Statistics of the last off-diagonal build, per quartet class (21 classes
+ * over the pair types SS, LS, LL, DS, DL, DD; class c pairs types (i,j),
+ * i <= j, enumerated row by row): screened-in shell quartets, quartets that
+ * passed the max|e| post-screen, primitive quartets evaluated, FP32 quartets
+ * (mixed form), and the kernel time in ms (0 unless timing is enabled). */
+int hfgpu_get_class_stats(const hfgpu_handle* h, long long* n_pass, long long* n_scattered,
+                          long long* n_prim, long long* n_fp32, double* ms);
+
+/* Enable (1) or disable (0) per-class CUDA-event timing of the off-diagonal
+ * kernels. */
+int hfgpu_set_timing(hfgpu_handle* h, int on);
+
+/* The CUDA stream the handle enqueues on (a cudaStream_t). */
+void* hfgpu_stream(hfgpu_handle* h);
+
+/* Measures the FP64 and FP32 FMA throughput of the current device (GFLOP/s,
+ * an FMA counted as 2) with an FMA-chain kernel; the denominators of the
+ * Fock kernels' roofline.  No reference counterpart. */
+int hfgpu_measure_fma_peak(double* fp64_gflops, double* fp32_gflops);
+
+/* One-electron integrals S, T, V (nb x nb, symmetric) over the basis, with
+ * the nuclei of charges[natom] at xyz[3*natom] (bohr).  Host code; replaces
+ * cmpt1e.f90 / one_electron_terms.f90 (set-up, off the Fock-build path).
+ * Any of S, T, V may be NULL. */
+int hfgpu_one_electron(const hfgpu_basis* basis, int natom, const double* charges, const double* xyz,
+                       double* S, double* T, double* V);
+
+/* Releases all device memory of the handle (dealloc_integs.f90's role). */
+int hfgpu_finalize(hfgpu_handle* h);
+
+/* Text of the last error on the calling thread ("" if none). */
+const char* hfgpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

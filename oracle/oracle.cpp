@@ -619,7 +619,7 @@ struct Oracle {
         add_sym(F, G.data(), nb);
     }
 
-    void non_diag(double* F, const double* P, double thr, int jonly) {
+    void non_diag(double* F, const double* P, double thr, int jonly, int stride = 1, int offset = 0) {
         std::vector<double> md;
         maxdm(P, md);
         std::vector<double> G((size_t)nb * nb, 0.0);
@@ -636,6 +636,7 @@ struct Oracle {
                     std::vector<double> e(625);
 #pragma omp for schedule(dynamic)
                     for (int ii = (ca == cb ? 1 : 0); ii < la; ++ii) {
+                        if (ii % stride != offset) continue;  // bounded CPU-baseline sample
                         int p1 = order[ca][ii];
                         int s1 = pairs[p1].sh1, s2 = pairs[p1].sh2;
                         int jend = (ca == cb) ? ii : lb;
@@ -742,6 +743,15 @@ int orc_fock_build_non_diag_j_only(void* h, double* f, const double* p, double t
     if (!o->have_schwarz) return 1;
     o->non_diag(f, p, thr, 1);
     return 0;
+}
+
+// Sampled off-diagonal build for the CPU baseline: only bra rows
+// ii % stride == offset of every class block; returns the screened-in count.
+long long orc_fock_build_non_diag_sample(void* h, double* f, const double* p, double thr, int stride, int offset) {
+    Oracle* o = (Oracle*)h;
+    if (!o->have_schwarz) return -1;
+    o->non_diag(f, p, thr, 0, stride, offset);
+    return o->n_screen_pass;
 }
 
 // Schwarz state left by fock_build_initial_diag: schw by (sh1,sh2) in an

@@ -44,6 +44,8 @@ def _lib():
     lib.orc_counts.argtypes = [vp, ll, ll]
     lib.orc_maxdm.argtypes = [vp, d, d]
     lib.orc_num_threads.restype = ctypes.c_int
+    lib.orc_fock_build_non_diag_sample.argtypes = [vp, d, d, ctypes.c_double, ctypes.c_int, ctypes.c_int]
+    lib.orc_fock_build_non_diag_sample.restype = ctypes.c_longlong
     return lib
 
 
@@ -108,6 +110,13 @@ class Oracle:
         pp = np.ascontiguousarray(p)
         if lib().orc_fock_build_non_diag_j_only(self.h, _dp(f), _dp(pp), thr) != 0:
             raise RuntimeError("fock_build_non_diag_j_only before fock_build_initial_diag")
+
+    def fock_build_non_diag_sample(self, f, p, thr, stride, offset=0):
+        pp = np.ascontiguousarray(p)
+        n = lib().orc_fock_build_non_diag_sample(self.h, _dp(f), _dp(pp), thr, stride, offset)
+        if n < 0:
+            raise RuntimeError("sample before fock_build_initial_diag")
+        return int(n)
 
     def eri(self, s1, s2, s3, s4):
         out = np.zeros(625)

@@ -1,0 +1,34 @@
+"""Shared fixtures of the test-suite: molecules, shells and densities."""
+from __future__ import annotations
+
+import functools
+
+import numpy as np
+
+from hfcode_b200 import basis, molecules
+
+
+@functools.lru_cache(maxsize=None)
+def system(name: str):
+    if name == "water":
+        mol, bas = molecules.water(), basis.load_basis("STO-3G")
+    elif name == "benzene":
+        mol, bas = molecules.benzene(), basis.load_basis("6-31G(d)")
+    elif name == "c60":
+        mol, bas = molecules.c60(), basis.load_basis("6-31G(d)")
+    elif name.startswith("alkane"):
+        mol, bas = molecules.alkane(int(name[6:])), basis.load_basis("6-31G(d)")
+    elif name.startswith("wc"):
+        k = int(name[2:])
+        mol, bas = molecules.water_cluster(k, np.random.default_rng(20261203 + k)), basis.load_basis("6-31G(d)")
+    else:
+        raise KeyError(name)
+    sh = basis.spread_basis(mol, bas)
+    p0 = basis.density_superposition(mol, bas, sh.nb)
+    return mol, bas, sh, p0
+
+
+def perturbed_density(p0: np.ndarray, seed: int, scale: float = 0.05) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    d = rng.normal(size=p0.shape) * scale
+    return p0 + 0.5 * (d + d.T)

@@ -1,0 +1,114 @@
+"""CUDA Fock builds against the CPU oracle, through the C ABI.
+
+Tolerance: 1e-10 absolute on every Fock element (the FP64 contract), on the
+same inputs.  Both sides apply the reference's screening, so the per-class
+counts of screened-in quartets must agree as well.
+"""
+import numpy as np
+import pytest
+
+from helpers import perturbed_density, system
+from oracle import pyoracle
+
+TOL = 1e-10
+REF2GPU = {0: 0, 3: 1, 9: 2, 2: 3, 8: 4, 7: 5}  # ss sl ll sd dl dd -> SS LS LL DS DL DD
+
+
+def gpu_class(ti, tj):
+    a, b = min(ti, tj), max(ti, tj)
+    c = 0
+    for i in range(6):
+        for j in range(i, 6):
+            if (i, j) == (a, b):
+                return c
+            c += 1
+
+
+def oracle_counts_by_gpu_class(orc):
+    passed, _ = orc.counts()
+    out = np.zeros(21, dtype=np.int64)
+    for ca in range(10):
+        for cb in range(10):
+            if passed[ca, cb]:
+                out[gpu_class(REF2GPU[ca], REF2GPU[cb])] += passed[ca, cb]
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["water", "alkane1", "alkane2", "benzene"])
+def test_fock_build_parity(name):
+    from hfcode_b200.fock import FockBuilder
+    _, _, sh, p0 = system(name)
+    nb = sh.nb
+    fb = FockBuilder(sh)
+    orc = pyoracle.Oracle(sh)
+    h = np.random.default_rng(1).normal(size=(nb, nb))
+    h = h + h.T
+    thr = 1e-10
+    # cycle 1: initial diag + non-diag
+    fg, fo = h.copy(order="F"), h.copy(order="F")
+    fb.fock_build_initial_diag(fg, p0, thr)
+    orc.fock_build_initial_diag(fo, p0, thr)
+    assert np.max(np.abs(fg - fo)) < TOL
+    sg, lastg = fb.schwarz()
+    so, lasto = orc.schwarz()
+    assert lastg == lasto
+    assert np.max(np.abs(sg - so)) < 1e-12
+    fb.fock_build_non_diag(fg, p0, thr)
+    orc.fock_build_non_diag(fo, p0, thr)
+    assert np.max(np.abs(fg - fo)) < TOL
+    st = fb.class_stats()
+    assert np.array_equal(st["pass"], oracle_counts_by_gpu_class(orc))
+    # later cycle: diag + non-diag on another density, and the incremental
+    # (delta-P, thr/10) build of direct_hartreefock.f90:111-121
+    p1 = perturbed_density(p0, 2)
+    fg, fo = h.copy(order="F"), h.copy(order="F")
+    fb.fock_build_diag(fg, p1, thr)
+    orc.fock_build_diag(fo, p1, thr)
+    assert np.max(np.abs(fg - fo)) < TOL
+    fb.fock_build_non_diag(fg, p1, thr)
+    orc.fock_build_non_diag(fo, p1, thr)
+    assert np.max(np.abs(fg - fo)) < TOL
+    dp = p1 - p0
+    dg, do = np.zeros((nb, nb)), np.zeros((nb, nb))
+    fb.fock_build_diag(dg, dp, thr)
+    orc.fock_build_diag(do, dp, thr)
+    fb.fock_build_non_diag(dg, dp, thr * 0.1)
+    orc.fock_build_non_diag(do, dp, thr * 0.1)
+    assert np.max(np.abs(dg - do)) < TOL
+    # J only
+    jg, jo = np.zeros((nb, nb)), np.zeros((nb, nb))
+    fb.fock_build_non_diag_j_only(jg, p1, thr)
+    orc.fock_build_non_diag_j_only(jo, p1, thr)
+    assert np.max(np.abs(jg - jo)) < TOL
+    fb.close()
+
+
+@pytest.mark.gpu
+def test_fock_build_is_symmetric_and_accumulates():
+    from hfcode_b200.fock import FockBuilder
+    _, _, sh, p0 = system("benzene")
+    fb = FockBuilder(sh)
+    nb = sh.nb
+    f1 = np.zeros((nb, nb))
+    fb.fock_build_initial_diag(f1, p0, 1e-10)
+    fb.fock_build_non_diag(f1, p0, 1e-10)
+    assert np.max(np.abs(f1 - f1.T)) < 1e-13
+    f2 = np.full((nb, nb), 3.0)
+    fb.fock_build_diag(f2, p0, 1e-10)
+    fb.fock_build_non_diag(f2, p0, 1e-10)
+    f3 = np.zeros((nb, nb))
+    fb.fock_build_diag(f3, p0, 1e-10)
+    fb.fock_build_non_diag(f3, p0, 1e-10)
+    assert np.max(np.abs(f2 - 3.0 - f3)) < 1e-12
+    fb.close()
+
+
+@pytest.mark.gpu
+def test_calls_before_initial_diag_are_rejected():
+    from hfcode_b200.fock import FockBuilder, HfgpuError
+    _, _, sh, p0 = system("water")
+    fb = FockBuilder(sh)
+    with pytest.raises(HfgpuError):
+        fb.fock_build_non_diag(np.zeros((sh.nb, sh.nb)), p0, 1e-10)
+    fb.close()
