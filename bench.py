@@ -276,7 +276,11 @@ def main():
             "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf, "traffic": None,
             "peak_source": "measured FP64 FMA-chain probe on this device (MEASURED_PEAKS.json has no FP64 figure)",
             "all_classes_tflops": float(cls_flops.sum() / (st["ms"].sum() * 1e-3) / 1e12),
-            "class_ms": {fock.CLASS_NAMES[c]: round(float(st["ms"][c]), 3) for c in range(21) if st["ms"][c] > 0}}
+            "class_ms": {fock.CLASS_NAMES[c]: round(float(st["ms"][c]), 3) for c in range(21) if st["ms"][c] > 0},
+            "class_tflops": {fock.CLASS_NAMES[c]: round(float(cls_flops[c] / (st["ms"][c] * 1e-3) / 1e12), 3)
+                             for c in range(21) if st["ms"][c] > 0},
+            "class_quartets": {fock.CLASS_NAMES[c]: int(st["pass"][c]) for c in range(21) if st["pass"][c] > 0},
+            "class_prim_quartets": {fock.CLASS_NAMES[c]: int(st["prim"][c]) for c in range(21) if st["prim"][c] > 0}}
     out = {"metric": METRIC, "value": value, "unit": "builds/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",

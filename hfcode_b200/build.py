@@ -50,13 +50,15 @@ def build(jobs: int = 0, verbose: bool = True) -> str:
         sys.path.pop(0)
     gen_srcs = gen_eri.main(os.path.join(CSRC, "generated"))
     os.makedirs(BUILD, exist_ok=True)
-    common = [os.path.join(CSRC, "common.cuh"), os.path.join(HERE, "..", "include", "hfgpu.h"),
+    common = [os.path.join(CSRC, "common.cuh"), os.path.join(CSRC, "types.cuh"), os.path.join(CSRC, "pairs.hpp"),
+              os.path.join(HERE, "..", "include", "hfgpu.h"),
               os.path.join(HERE, "..", "include", "hfgpu_basis.h")]
     srcs = [os.path.join(CSRC, "hfgpu.cu"), os.path.join(CSRC, "onee.cpp")] + sorted(gen_srcs)
     objs = [os.path.join(BUILD, os.path.splitext(os.path.basename(s))[0] + ".o") for s in srcs]
     jobs = jobs or max(1, min(len(srcs), os.cpu_count() or 4))
     with cf.ThreadPoolExecutor(jobs) as ex:
-        futs = [ex.submit(_compile, s, o, common) for s, o in zip(srcs, objs)]
+        futs = [ex.submit(_compile, s, o, common + ([s[:-3] + ".cuh"] if os.path.exists(s[:-3] + ".cuh") else []))
+                for s, o in zip(srcs, objs)]
         for f in futs:
             done = f.result()
             if done and verbose:

@@ -4,93 +4,12 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "types.cuh"
+
 #include <cstdint>
 #include <type_traits>
 
 namespace hfgpu {
-
-constexpr double INTTHRESH = 1e-10;     // molprops.f90:162
-constexpr int NPT = 6;                  // GPU pair types SS LS LL DS DL DD
-constexpr int NCLS = 21;                // quartet classes over the pair types
-constexpr int BOYS_NPT = 225;           // grid T_j = j/8, j = 0..224 (T <= 28)
-constexpr int BOYS_K = 8;               // Taylor terms per grid point
-constexpr int BOYS_MMAX = 8;            // highest order used: (dd|dd)
-
-// Primitive pair (one surviving primitive product of a shell pair): exponent
-// sum p, centre P, K_ab = sqrt(2 pi^2.5) exp(-ab/p r^2)/p d_a d_b
-// (precalc_kabs.f90:103-109) and the L-shell p/s ratios of both primitives.
-struct GPrim {
-    double p;
-    double P[3];
-    double K;
-    double w1, w2;
-    double pad;
-};
-
-// Shell pair in GPU orientation (larger shell first).
-struct GPair {
-    double A[3];
-    double B[3];
-    int p0, np;    // range in the primitive-pair array
-    int sa, sb;    // shell indices
-    int aoa, aob;  // first AO of each shell
-};
-
-// ---------------------------------------------------------------- Boys ----
-// F_m(T) for m = 0..M.  T > 28: F_0 = sqrt(pi/T)/2 and upward recursion
-// without the exponential, which is what the reference evaluates there
-// (boys.f90:134-139).  T <= 28: 8-term Taylor expansion of F_M about the
-// nearest point of a 1/8-spaced grid (coefficients F_{M+k}(T_j)(-1)^k/k!
-// staged in shared memory), then downward recursion
-// F_m = (2T F_{m+1} + e^-T)/(2m+1).
-template <int M>
-__device__ __forceinline__ void boys_eval(double T, const double* __restrict__ tab, double* F) {
-    if (T > 28.0) {
-        const double it = 1.0 / T;
-        F[0] = 0.88622692545275801365 * sqrt(it);
-#pragma unroll
-        for (int m = 1; m <= M; ++m) F[m] = F[m - 1] * ((m - 0.5) * it);
-    } else {
-        const int j = __double2int_rn(T * 8.0);
-        const double x = T - 0.125 * j;
-        const double* c = tab + j * BOYS_K;
-        double f = c[BOYS_K - 1];
-#pragma unroll
-        for (int k = BOYS_K - 2; k >= 0; --k) f = fma(f, x, c[k]);
-        F[M] = f;
-        if (M > 0) {
-            const double e = exp(-T);
-            const double t2 = T + T;
-#pragma unroll
-            for (int m = M - 1; m >= 0; --m) F[m] = fma(t2, F[m + 1], e) * (1.0 / (2 * m + 1));
-        }
-    }
-}
-
-template <int M>
-__device__ __forceinline__ void boys_eval(float T, const float* __restrict__ tab, float* F) {
-    if (T > 28.0f) {
-        const float it = 1.0f / T;
-        F[0] = 0.886226925f * sqrtf(it);
-#pragma unroll
-        for (int m = 1; m <= M; ++m) F[m] = F[m - 1] * ((m - 0.5f) * it);
-    } else {
-        const int j = __float2int_rn(T * 8.0f);
-        const float x = T - 0.125f * j;
-        const float* c = tab + j * BOYS_K;
-        float f = c[5];
-#pragma unroll
-        for (int k = 4; k >= 0; --k) f = fmaf(f, x, c[k]);
-        F[M] = f;
-        if (M > 0) {
-            const float e = __expf(-T);
-            const float t2 = T + T;
-#pragma unroll
-            for (int m = M - 1; m >= 0; --m) F[m] = fmaf(t2, F[m + 1], e) * (1.0f / (2 * m + 1));
-        }
-    }
-}
-
 
 // ------------------------------------------------------- class traits ----
 __host__ __device__ constexpr int pt_na(int t) { return t == 0 ? 1 : t == 1 ? 4 : t == 2 ? 4 : 5; }
@@ -362,6 +281,8 @@ typedef void (*DiagKernel)(DiagArgs);
 struct ClassKernels {
     NDKernel nd64, nd32;
     DiagKernel diag0, diag1;  // only for classes (X|X)
+    int nd_threads, nd_qpb;   // block size and quartets per block
+    int dg_threads, dg_ppb;   // block size and pairs per block (diag)
     int bi, ki, L, nout;
 };
 

@@ -142,7 +142,7 @@ class VRR:
                 terms.append(f"h2q{f1[i]}*({self.get(e, f2, m)} - rq*{self.get(e, f2, m + 1)})")
             if e[i] > 0:
                 e1 = add(e, i, -1)
-                terms.append(f"h2pq{e[i]}*{self.get(e1, f, m + 1)}")
+                terms.append(f"h2pq{e[i]}*{self.get(e1, f1, m + 1)}")
         self.nops += len(terms)
         name = self.em.tmp(" + ".join(terms), "v")
         self.nodes[key] = name
@@ -174,6 +174,8 @@ def comps(t: str):
 
 
 class ClassGen:
+    """Code generator of one quartet class (A B|C D), GPU shell order."""
+
     def __init__(self, bra: Tuple[str, str], ket: Tuple[str, str], ftype="double", suffix=""):
         self.A, self.B = bra
         self.C, self.D = ket
@@ -182,79 +184,148 @@ class ClassGen:
         self.L = LMAX[self.A] + LMAX[self.B] + LMAX[self.C] + LMAX[self.D]
         self.bra_combos = sub_combos(self.A, self.B)
         self.ket_combos = sub_combos(self.C, self.D)
+        self.types = [self.A, self.B, self.C, self.D]
+        self.cl = [comps(t) for t in self.types]
+        self.nf = [NFUNC[t] for t in self.types]
+        self.outputs = list(itertools.product(*[range(n) for n in self.nf]))
+        self._leaf_cache: Dict[Tuple, frozenset] = {}
+
+    @property
+    def tag(self):
+        return f"{self.A}{self.B}_{self.C}{self.D}"
 
     @property
     def name(self):
-        return f"eri_{self.A}{self.B}_{self.C}{self.D}{self.suffix}"
+        return f"eri_{self.tag}{self.suffix}"
 
     @property
     def nout(self):
-        return NFUNC[self.A] * NFUNC[self.B] * NFUNC[self.C] * NFUNC[self.D]
+        return len(self.outputs)
 
-    def targets(self):
-        t = set()
-        for (la, lb, _) in self.bra_combos:
-            for (lc, ld, _) in self.ket_combos:
-                for de in range(la, la + lb + 1):
-                    for df in range(lc, lc + ld + 1):
-                        for e in carts(de):
-                            for f in carts(df):
-                                t.add((e, f))
-        return sorted(t)
+    # ---------------------------------------------------------------- deps
+    def cart_terms(self, o):
+        """Output function (i,j,k,l) as sum of coef * Cartesian (ca,cb,cc,cd)."""
+        per = []
+        for ax, t in enumerate(self.types):
+            if t == "D":
+                per.append(HARM[o[ax]])
+            else:
+                per.append([(1.0, o[ax])])
+        out = []
+        for combo in itertools.product(*per):
+            c = 1.0
+            idx = []
+            for coef, ci in combo:
+                c *= coef
+                idx.append(ci)
+            out.append((c, tuple(idx)))
+        return out
 
-    def gen_vrr(self, order):
-        em = Emitter(self.ft)
-        v = VRR(em, order)
-        for (e, f) in self.targets():
-            v.get(e, f, 0)
-        return em, v
+    def combo_of(self, cart4):
+        sa, sb, sc, sd = (self.cl[ax][cart4[ax]][0] for ax in range(4))
+        la, lb = SUBS[self.A][sa][0], SUBS[self.B][sb][0]
+        lc, ld = SUBS[self.C][sc][0], SUBS[self.D][sd][0]
+        bi = next(i for i, x in enumerate(self.bra_combos) if x[0] == la and x[1] == lb)
+        ki = next(i for i, x in enumerate(self.ket_combos) if x[0] == lc and x[1] == ld)
+        return bi, ki
 
-    def emit(self) -> str:
+    def leaves(self, cart4) -> frozenset:
+        """Accumulator keys (bi, ki, e, f) the HRR of one Cartesian quartet reads."""
+        if cart4 in self._leaf_cache:
+            return self._leaf_cache[cart4]
+        bi, ki = self.combo_of(cart4)
+        a, b, c, d = (self.cl[ax][cart4[ax]][1] for ax in range(4))
+        out = set()
+
+        def ket(e, c, d):
+            if d == Z3:
+                out.add((bi, ki, e, c))
+                return
+            i = max(range(3), key=lambda k: (d[k], -k))
+            d1 = add(d, i, -1)
+            ket(e, add(c, i), d1)
+            ket(e, c, d1)
+
+        def bra(a, b):
+            if b == Z3:
+                ket(a, c, d)
+                return
+            i = max(range(3), key=lambda k: (b[k], -k))
+            b1 = add(b, i, -1)
+            bra(add(a, i), b1)
+            bra(a, b1)
+
+        bra(a, b)
+        r = frozenset(out)
+        self._leaf_cache[cart4] = r
+        return r
+
+    def out_leaves(self, o):
+        s = set()
+        for _, c4 in self.cart_terms(o):
+            s |= self.leaves(c4)
+        return s
+
+    def partition(self, acc_max: int, out_max: int):
+        """Greedy split of the outputs (flat order) into roles whose
+        accumulator and output counts fit the register budget."""
+        groups, cur, cur_acc = [], [], set()
+        for n, o in enumerate(self.outputs):
+            lv = self.out_leaves(o)
+            if cur and (len(cur_acc | lv) > acc_max or len(cur) >= out_max):
+                groups.append(cur)
+                cur, cur_acc = [], set()
+            cur.append(n)
+            cur_acc |= lv
+        if cur:
+            groups.append(cur)
+        return groups
+
+    # ---------------------------------------------------------------- emit
+    def emit_role(self, fname: str, outs: List[int]):
+        """Device function computing the outputs `outs` (flat indices) into
+        out[0..len(outs)).  Returns (code, stats)."""
         ft = self.ft
         dbl = ft == "double"
-        # choose the cheaper VRR order
-        em_b, v_b = self.gen_vrr("bra")
-        em_k, v_k = self.gen_vrr("ket")
-        em, vrr = (em_b, v_b) if v_b.nops <= v_k.nops else (em_k, v_k)
         L = self.L
-        # FLOP model (an FMA counts 2): per primitive quartet the set-up (~40),
-        # Boys (Taylor 7 FMA + 2 per downward step), every VRR term (one FMA,
-        # plus one for each (x - rho/p y) bracket) and every accumulation FMA;
-        # per contracted quartet the HRR/spherical adds and the J/K scatter
-        # (6 FMA per function quartet).
-        nbracket = sum(line.count(" - r") for line in em.lines)
-        nacc = sum(len(carts(de)) * len(carts(df))
-                   for (la, lb, _) in self.bra_combos for (lc, ld, _) in self.ket_combos
-                   for de in range(la, la + lb + 1) for df in range(lc, lc + ld + 1))
-        self.flops_prim = 40 + 14 + 4 * L + 2 * vrr.nops + 2 * nbracket + 2 * nacc
-        self.nvrr = vrr.nops
+        cv = (lambda s: s) if dbl else (lambda s: f"(float)({s})")
+        needed_acc = set()
+        for n in outs:
+            needed_acc |= self.out_leaves(self.outputs[n])
+        targets = sorted({(e, f) for (_, _, e, f) in needed_acc})
+
+        def gen_vrr(order):
+            em = Emitter(ft)
+            v = VRR(em, order)
+            for (e, f) in targets:
+                v.get(e, f, 0)
+            return em, v
+
+        em_b, v_b = gen_vrr("bra")
+        em_k, v_k = gen_vrr("ket")
+        em, vrr = (em_b, v_b) if v_b.nops <= v_k.nops else (em_k, v_k)
+        acc = {}
+        for key in sorted(needed_acc, key=lambda k: (k[0], k[1], sum(k[2]), k[2], sum(k[3]), k[3])):
+            bi, ki, e, f = key
+            acc[key] = f"a{bi}{ki}_{''.join(map(str, e))}_{''.join(map(str, f))}"
         out = []
         w = out.append
-        w(f"// class ({self.A}{self.B}|{self.C}{self.D}): L={L}, {self.nout} functions, "
-          f"VRR {vrr.nops} terms ({vrr.order}-first)")
-        w(f"__device__ __forceinline__ void {self.name}(const GPair& bra, const GPair& ket,")
+        w(f"// ({self.A}{self.B}|{self.C}{self.D}) outputs {outs[0]}..{outs[-1]} ({len(outs)}): L={L}, "
+          f"{len(acc)} accumulators, VRR {vrr.nops} terms ({vrr.order}-first)")
+        w(f"__device__ __forceinline__ void {fname}(const GPair& bra, const GPair& ket,")
         w(f"    const GPrim* __restrict__ prims, const {ft}* __restrict__ btab, {ft}* __restrict__ out)")
         w("{")
-        # accumulators
-        acc = {}
-        for bi, (la, lb, _) in enumerate(self.bra_combos):
-            for ki, (lc, ld, _) in enumerate(self.ket_combos):
-                for de in range(la, la + lb + 1):
-                    for df in range(lc, lc + ld + 1):
-                        for e in carts(de):
-                            for f in carts(df):
-                                nm = f"a{bi}{ki}_{''.join(map(str, e))}_{''.join(map(str, f))}"
-                                acc[(bi, ki, e, f)] = nm
         w(f"    {ft} " + ", ".join(f"{n} = 0" for n in acc.values()) + ";")
-        cv = (lambda s: s) if dbl else (lambda s: f"(float)({s})")
-        w(f"    const double Ax = bra.A[0], Ay = bra.A[1], Az = bra.A[2];")
-        w(f"    const double Cx = ket.A[0], Cy = ket.A[1], Cz = ket.A[2];")
+        w("    const double Ax = bra.A[0], Ay = bra.A[1], Az = bra.A[2];")
+        w("    const double Cx = ket.A[0], Cy = ket.A[1], Cz = ket.A[2];")
         w("    for (int ib = 0; ib < bra.np; ++ib) {")
         w("        const GPrim pb = prims[bra.p0 + ib];")
         w(f"        const {ft} p = {cv('pb.p')};")
         w(f"        const {ft} PA0 = {cv('pb.P[0] - Ax')}, PA1 = {cv('pb.P[1] - Ay')}, PA2 = {cv('pb.P[2] - Az')};")
-        # bra combo weights
-        for bi, (_, _, wt) in enumerate(self.bra_combos):
+        used_b = sorted({k[0] for k in acc})
+        used_k = sorted({k[1] for k in acc})
+        for bi in used_b:
+            wt = self.bra_combos[bi][2]
             expr = " * ".join(cv(f"pb.w{x}") for x in wt) if wt else "1"
             w(f"        const {ft} wb{bi} = {expr};")
         w("        for (int ik = 0; ik < ket.np; ++ik) {")
@@ -267,7 +338,8 @@ class ClassGen:
         if dbl:
             w("            const double PQ0 = pb.P[0] - pk.P[0], PQ1 = pb.P[1] - pk.P[1], PQ2 = pb.P[2] - pk.P[2];")
         else:
-            w("            const float PQ0 = (float)(pb.P[0] - pk.P[0]), PQ1 = (float)(pb.P[1] - pk.P[1]), PQ2 = (float)(pb.P[2] - pk.P[2]);")
+            w("            const float PQ0 = (float)(pb.P[0] - pk.P[0]), PQ1 = (float)(pb.P[1] - pk.P[1]), "
+              "PQ2 = (float)(pb.P[2] - pk.P[2]);")
         w(f"            const {ft} T = rho * (PQ0 * PQ0 + PQ1 * PQ1 + PQ2 * PQ2);")
         w(f"            {ft} F[{L + 1}];")
         w(f"            boys_eval<{L}>(T, btab, F);")
@@ -278,25 +350,25 @@ class ClassGen:
         for m in range(L + 1):
             w(f"            const {ft} B{m} = pref * F[{m}];")
         if L > 0:
-            # W - P = -q/(p+q) * (P - Q) ; W - Q = p/(p+q) * (P - Q)
             w(f"            const {ft} qo = q * opq, po = p * opq;")
             w(f"            const {ft} WP0 = -qo * PQ0, WP1 = -qo * PQ1, WP2 = -qo * PQ2;")
             w(f"            const {ft} WQ0 = po * PQ0, WQ1 = po * PQ1, WQ2 = po * PQ2;")
             if dbl:
                 w("            const double QC0 = pk.P[0] - Cx, QC1 = pk.P[1] - Cy, QC2 = pk.P[2] - Cz;")
             else:
-                w("            const float QC0 = (float)(pk.P[0] - Cx), QC1 = (float)(pk.P[1] - Cy), QC2 = (float)(pk.P[2] - Cz);")
+                w("            const float QC0 = (float)(pk.P[0] - Cx), QC1 = (float)(pk.P[1] - Cy), "
+                  "QC2 = (float)(pk.P[2] - Cz);")
             w(f"            const {ft} h2p1 = {half} / p, rp = rho / p;")
             w(f"            const {ft} h2q1 = {half} / q, rq = rho / q;")
             w(f"            const {ft} h2pq1 = {half} * opq;")
             for n in range(2, 5):
                 w(f"            const {ft} h2p{n} = {n} * h2p1, h2q{n} = {n} * h2q1, h2pq{n} = {n} * h2pq1;")
-        for ki, (_, _, wt) in enumerate(self.ket_combos):
+        for ki in used_k:
+            wt = self.ket_combos[ki][2]
             expr = " * ".join(cv(f"pk.w{x}") for x in wt) if wt else "1"
             w(f"            const {ft} wk{ki} = {expr};")
         for line in em.lines:
             w("        " + line)
-        # accumulate
         for (bi, ki, e, f), nm in acc.items():
             src = vrr.nodes[(e, f, 0)]
             wexp = []
@@ -304,17 +376,15 @@ class ClassGen:
                 wexp.append(f"wb{bi}")
             if self.ket_combos[ki][2]:
                 wexp.append(f"wk{ki}")
-            if wexp:
-                w(f"            {nm} += {' * '.join(wexp)} * {src};")
-            else:
-                w(f"            {nm} += {src};")
+            w(f"            {nm} += {' * '.join(wexp + [src])};")
         w("        }")
         w("    }")
-        # HRR
+        w(f"    const {ft} AB0 = {cv('bra.A[0] - bra.B[0]')}, AB1 = {cv('bra.A[1] - bra.B[1]')}, "
+          f"AB2 = {cv('bra.A[2] - bra.B[2]')};")
+        w(f"    const {ft} CD0 = {cv('ket.A[0] - ket.B[0]')}, CD1 = {cv('ket.A[1] - ket.B[1]')}, "
+          f"CD2 = {cv('ket.A[2] - ket.B[2]')};")
         hem = Emitter(ft)
         memo = {}
-        w(f"    const {ft} AB0 = {cv('bra.A[0] - bra.B[0]')}, AB1 = {cv('bra.A[1] - bra.B[1]')}, AB2 = {cv('bra.A[2] - bra.B[2]')};")
-        w(f"    const {ft} CD0 = {cv('ket.A[0] - ket.B[0]')}, CD1 = {cv('ket.A[1] - ket.B[1]')}, CD2 = {cv('ket.A[2] - ket.B[2]')};")
 
         def ket_hrr(bi, ki, e, c, d):
             key = ("k", bi, ki, e, c, d)
@@ -346,68 +416,267 @@ class ClassGen:
             memo[key] = r
             return r
 
-        # Cartesian results per component tuple
-        cart = {}
-        CA, CB, CC, CDc = comps(self.A), comps(self.B), comps(self.C), comps(self.D)
-        for ia, (sa, ca) in enumerate(CA):
-            for ib, (sb, cb) in enumerate(CB):
-                bi = self.bra_combos.index(next(x for x in self.bra_combos if x[0] == SUBS[self.A][sa][0] and x[1] == SUBS[self.B][sb][0]))
-                for ic, (sc, cc) in enumerate(CC):
-                    for id_, (sd, cd) in enumerate(CDc):
-                        ki = self.ket_combos.index(next(x for x in self.ket_combos if x[0] == SUBS[self.C][sc][0] and x[1] == SUBS[self.D][sd][0]))
-                        cart[(ia, ib, ic, id_)] = bra_hrr(bi, ki, ca, cb, cc, cd)
+        def cart_val(c4):
+            bi, ki = self.combo_of(c4)
+            a, b, c, d = (self.cl[ax][c4[ax]][1] for ax in range(4))
+            return bra_hrr(bi, ki, a, b, c, d)
+
+        sph = []
+        nsph = 0
+        for r, n in enumerate(outs):
+            terms = []
+            for coef, c4 in self.cart_terms(self.outputs[n]):
+                v = cart_val(c4)
+                terms.append(v if coef == 1.0 else f"{fmt_coef(coef, ft)}*{v}")
+            nsph += len(terms) - 1
+            sph.append(f"    out[{r}] = {' + '.join(terms)};")
         for line in hem.lines:
             w(line)
-        self.nhrr = len(hem.lines)
-        # spherical transform of d shells, centre by centre
-        dims = [len(CA), len(CB), len(CC), len(CDc)]
-        types = [self.A, self.B, self.C, self.D]
-        sem = Emitter(ft)
-        cur = cart
-        for ax in range(4):
-            if types[ax] != "D":
-                continue
-            nxt = {}
-            rng = [range(d) for d in dims]
-            rng[ax] = range(5)
-            for idx in itertools.product(*rng):
-                terms = []
-                for coef, cc in HARM[idx[ax]]:
-                    src = list(idx)
-                    src[ax] = cc
-                    v = cur[tuple(src)]
-                    terms.append(v if coef == 1.0 else f"{fmt_coef(coef, ft)}*{v}")
-                nxt[idx] = sem.tmp(" + ".join(terms), "s")
-            dims[ax] = 5
-            cur = nxt
-        for line in sem.lines:
-            w(line)
-        nsph = sum(l.count("+") + 1 for l in sem.lines)
-        self.flops_quartet = 2 * self.nhrr + 2 * nsph + 12 * self.nout
-        n = 0
-        for idx in itertools.product(*[range(d) for d in dims]):
-            w(f"    out[{n}] = {cur[idx]};")
-            n += 1
-        assert n == self.nout
+        out.extend(sph)
         w("}")
-        return "\n".join(out)
+        nbracket = sum(line.count(" - r") for line in em.lines)
+        stats = {"vrr": vrr.nops, "bracket": nbracket, "acc": len(acc), "hrr": len(hem.lines), "sph": nsph}
+        return "\n".join(out), stats
+
+    def flop_model(self):
+        """Algorithmic FLOPs of the class in its single-function formulation
+        (an FMA counts 2): per primitive quartet the set-up (~40), Boys
+        (Taylor 7 FMA + 2 per downward step), every VRR term (one FMA, plus
+        one for each (x - rho/p y) bracket) and every accumulation FMA; per
+        contracted quartet the HRR/spherical adds and the J/K scatter (6 FMA
+        per function quartet)."""
+        _, st = self.emit_role("_count", list(range(self.nout)))
+        self.flops_prim = 40 + 14 + 4 * self.L + 2 * st["vrr"] + 2 * st["bracket"] + 2 * st["acc"]
+        self.flops_quartet = 2 * st["hrr"] + 2 * st["sph"] + 12 * self.nout
+        self.nvrr, self.nhrr = st["vrr"], st["hrr"]
+
+    # ------------------------------------------------------------- scatter
+    def emit_scatter(self, fname: str, outs: List[int]) -> str:
+        """J/K scatter of the outputs `outs` with uniform weight s into the
+        one-triangle buffer G (F += G + G^T later); P is column-major."""
+        o4 = [self.outputs[n] for n in outs]
+        lines = [f"template <typename E>",
+                 f"__device__ __forceinline__ void {fname}(const E* __restrict__ e, double s, const GPair& bra, "
+                 f"const GPair& ket, const double* __restrict__ P, double* __restrict__ G, int nb, bool jonly)",
+                 "{",
+                 "    const int a0 = bra.aoa, b0 = bra.aob, c0 = ket.aoa, d0 = ket.aob;",
+                 "    const double s2 = 2.0 * s, hs = -0.5 * s;"]
+        loaded = set()
+        org = {"a": "a0", "b": "b0", "c": "c0", "d": "d0"}
+
+        def pv(x, i, y, j):
+            nm = f"p{x}{i}{y}{j}"
+            if nm not in loaded:
+                loaded.add(nm)
+                lines.append(f"    const double {nm} = __ldg(P + ({org[x]} + {i}) + (size_t)({org[y]} + {j}) * nb);")
+            return nm
+
+        def block(rowx, rowi, colx, coli, px, pi, qx, qi, scale, tgt):
+            groups: Dict[Tuple[int, int], List[Tuple[int, int]]] = {}
+            for r, o in enumerate(o4):
+                key = (o[rowi], o[coli])
+                groups.setdefault(key, []).append((r, o))
+            for (i, j), lst in groups.items():
+                terms = [f"{pv(px, o[pi], qx, o[qi])} * (double)e[{r}]" for r, o in lst]
+                lines.append(f"    atomicAdd(G + ({org[rowx]} + {i}) + (size_t)({org[colx]} + {j}) * nb, "
+                             f"{scale} * ({' + '.join(terms)}));")
+
+        # J_ab <- P_cd, J_cd <- P_ab
+        block("a", 0, "b", 1, "c", 2, "d", 3, "s2", "J")
+        block("c", 2, "d", 3, "a", 0, "b", 1, "s2", "J")
+        lines.append("    if (jonly) return;")
+        # K_ac <- P_bd, K_ad <- P_bc, K_bc <- P_ad, K_bd <- P_ac
+        block("a", 0, "c", 2, "b", 1, "d", 3, "hs", "K")
+        block("a", 0, "d", 3, "b", 1, "c", 2, "hs", "K")
+        block("b", 1, "c", 2, "a", 0, "d", 3, "hs", "K")
+        block("b", 1, "d", 3, "a", 0, "c", 2, "hs", "K")
+        lines.append("}")
+        return "\n".join(lines)
 
 
-CLASS_TU = """// GENERATED by gen_eri.py -- do not edit.
-// Kernels of quartet class ({A}{B}|{C}{D}).
-#include "../common.cuh"
+ACC_MAX = 96
+OUT_MAX = 48
+MAX_ROLES = 10
+
+
+def class_source(ci: int, bi: int, ki: int):
+    """Header (device functions) and translation unit (kernels) of one
+    quartet class; returns (cuh_text, cu_text, info)."""
+    g = ClassGen(PAIR_TYPES[bi], PAIR_TYPES[ki], "double")
+    g.flop_model()
+    roles = g.partition(ACC_MAX, OUT_MAX)
+    if len(roles) > MAX_ROLES:  # d-heavy classes: one thread per quartet
+        roles = [list(range(g.nout))]
+    R = len(roles)
+    g32 = ClassGen(PAIR_TYPES[bi], PAIR_TYPES[ki], "float", suffix="_f32")
+    funcs = []
+    if R == 1:
+        code, _ = g.emit_role(g.name, roles[0])
+        code32, _ = g32.emit_role(g32.name, roles[0])
+        funcs += [code, code32]
+    else:
+        for r, outs in enumerate(roles):
+            code, _ = g.emit_role(f"{g.name}_r{r}", outs)
+            code32, _ = g32.emit_role(f"{g32.name}_r{r}", outs)
+            funcs += [code, code32, g.emit_scatter(f"scat_{g.tag}_r{r}", outs)]
+    cuh = CLASS_CUH.format(A=g.A, B=g.B, C=g.C, D=g.D, roles=R, body="\n\n".join(funcs))
+    info = {"name": f"{g.A}{g.B}|{g.C}{g.D}", "tag": g.tag, "L": g.L, "nout": g.nout, "roles": R,
+            "role_sizes": [len(x) for x in roles], "role_outs": roles,
+            "flops_prim": g.flops_prim, "flops_quartet": g.flops_quartet,
+            "vrr_terms": g.nvrr, "hrr_terms": g.nhrr}
+    if R == 1:
+        reg = (f"    k->nd64 = k_nondiag<Cls_{g.tag}, false>;\n"
+               f"    k->nd32 = k_nondiag<Cls_{g.tag}, true>;\n"
+               f"    k->nd_threads = ND_THREADS;\n    k->nd_qpb = ND_THREADS;\n")
+        if bi == ki:
+            reg += (f"    k->diag0 = k_diag<Cls_{g.tag}, 0>;\n    k->diag1 = k_diag<Cls_{g.tag}, 1>;\n"
+                    f"    k->dg_threads = ND_THREADS;\n    k->dg_ppb = ND_THREADS;\n")
+        kern = ""
+    else:
+        reg = (f"    k->nd64 = k_nd_{g.tag}<false>;\n    k->nd32 = k_nd_{g.tag}<true>;\n"
+               f"    k->nd_threads = {32 * R};\n    k->nd_qpb = 32;\n")
+        if bi == ki:
+            reg += (f"    k->diag0 = k_dg_{g.tag}<0>;\n    k->diag1 = k_dg_{g.tag}<1>;\n"
+                    f"    k->dg_threads = {32 * R};\n    k->dg_ppb = 32;\n")
+        kern = role_kernels(g, roles, bi == ki)
+    if bi != ki:
+        reg += "    k->diag0 = nullptr;\n    k->diag1 = nullptr;\n"
+    traits = (f"HF_CLASS_TRAITS({ci}, {bi}, {ki}, {g.tag}, {g.nout}, {g.L})\n" if R == 1 else "")
+    cu = CLASS_TU.format(A=g.A, B=g.B, C=g.C, D=g.D, kernels=kern, ci=ci, bi=bi, ki=ki, tag=g.tag,
+                         hdr=f"cls_{ci:02d}_{g.tag}.cuh", nout=g.nout, L=g.L, reg=reg, roles=R, traits=traits)
+    return cuh, cu, info
+
+
+def role_kernels(g: ClassGen, roles, diag: bool) -> str:
+    """Kernels of a class split into R roles: a block is R warps over 32
+    quartets; warp r evaluates role r of the quartet of its lane.  The
+    post-screen max|e| is reduced across the warps through shared memory."""
+    R = len(roles)
+    nmax = max(len(x) for x in roles)
+    tag, L = g.tag, g.L
+    cases = []
+    for r, outs in enumerate(roles):
+        cases.append(f"        case {r}: if constexpr (F32) eri_{tag}_f32_r{r}(bra, ket, a.prims, sboys, e); "
+                     f"else eri_{tag}_r{r}(bra, ket, a.prims, sboys, e); nloc = {len(outs)}; break;")
+    scat = [f"            case {r}: scat_{tag}_r{r}(e, s, bra, ket, a.P, a.G, a.nb, a.jonly); break;"
+            for r in range(R)]
+    txt = f"""
+template <bool F32>
+__global__ void __launch_bounds__({32 * R}) k_nd_{tag}(NDArgs a) {{
+    using Real = typename std::conditional<F32, float, double>::type;
+    __shared__ Real sboys[BOYS_NPT * BOYS_K];
+    __shared__ double smax[{32 * R}];
+    if constexpr (F32) stage_boys<{L}>(sboys, a.boysf);
+    else stage_boys<{L}>(sboys, a.boys);
+    const int lane = threadIdx.x & 31, role = threadIdx.x >> 5;
+    const int t = blockIdx.x * 32 + lane;
+    const bool valid = t < a.n;
+    const int tt = valid ? t : 0;
+    const uint2 q = a.from_back ? a.quartets[a.cap - 1 - tt] : a.quartets[tt];
+    const GPair bra = a.bra[q.x];
+    const GPair ket = a.ket[q.y];
+    Real e[{nmax}];
+    int nloc = 0;
+    double mx = 0.0;
+    if (valid) {{
+        switch (role) {{
+{chr(10).join(cases)}
+        }}
+#pragma unroll
+        for (int i = 0; i < {nmax}; ++i)
+            if (i < nloc) mx = fmax(mx, (double)fabs(e[i]));
+    }}
+    smax[threadIdx.x] = mx;
+    __syncthreads();
+    double g = 0.0;
+#pragma unroll
+    for (int r = 0; r < {R}; ++r) g = fmax(g, smax[r * 32 + lane]);
+    const bool keep = valid && !(g < a.thr);  // fock_build_non_diag.f90:69
+    if (keep) {{
+        const double s = (bra.sa == bra.sb ? 0.5 : 1.0) * (ket.sa == ket.sb ? 0.5 : 1.0);
+        switch (role) {{
+{chr(10).join(scat)}
+        }}
+    }}
+    if (a.stats && role == 0)
+        warp_add_stats(a.stats, keep ? 1ull : 0ull, valid ? (unsigned long long)(bra.np * ket.np) : 0ull,
+                       (F32 && keep) ? 1ull : 0ull);
+}}
+"""
+    if diag:
+        dcases = []
+        for r, outs in enumerate(roles):
+            dcases.append(f"        case {r}: eri_{tag}_r{r}(pr, pr, a.prims, sboys, e); nloc = {len(outs)}; break;")
+        txt += f"""
+template <int MODE>
+__global__ void __launch_bounds__({32 * R}) k_dg_{tag}(DiagArgs a) {{
+    __shared__ double sboys[BOYS_NPT * BOYS_K];
+    __shared__ double smax[{32 * R}];
+    stage_boys<{L}>(sboys, a.boys);
+    const int lane = threadIdx.x & 31, role = threadIdx.x >> 5;
+    const int t = blockIdx.x * 32 + lane;
+    bool valid = t < a.n;
+    const GPair pr = a.pairs[valid ? t : 0];
+    if (MODE == 1 && valid) {{
+        const double mv = fmax(a.md[pr.sa * a.nsh + pr.sb],
+                               fmax(0.25 * a.md[pr.sb * a.nsh + pr.sb], 0.25 * a.md[pr.sa * a.nsh + pr.sa]));
+        const double sw = a.schw[t];
+        if (sw * sw * mv < a.thr) valid = false;  // fock_build_diag.f90:20-21
+    }}
+    double e[{nmax}];
+    int nloc = 0;
+    double mx = 0.0;
+    if (valid) {{
+        switch (role) {{
+{chr(10).join(dcases)}
+        }}
+#pragma unroll
+        for (int i = 0; i < {nmax}; ++i)
+            if (i < nloc) mx = fmax(mx, fabs(e[i]));
+    }}
+    smax[threadIdx.x] = mx;
+    __syncthreads();
+    if (MODE == 0 && valid && role == 0) {{
+        double g = 0.0;
+#pragma unroll
+        for (int r = 0; r < {R}; ++r) g = fmax(g, smax[r * 32 + lane]);
+        a.schw[t] = sqrt(g);
+    }}
+    if (valid) {{
+#pragma unroll
+        for (int i = 0; i < {nmax}; ++i)
+            if (!(fabs(e[i]) > INTTHRESH)) e[i] = 0.0;  // element skip
+        const double f = pr.sa == pr.sb ? 1.0 : 2.0;
+        const double s = f * f / 8.0;
+        switch (role) {{
+{chr(10).join(f"            case {r}: scat_{tag}_r{r}(e, s, pr, pr, a.P, a.G, a.nb, false); break;" for r in range(R))}
+        }}
+    }}
+}}
+"""
+    return txt
+
+
+CLASS_CUH = """// GENERATED by gen_eri.py -- do not edit.
+// Device functions of quartet class ({A}{B}|{C}{D}): {roles} role(s).
+#pragma once
+#include "../types.cuh"
 
 namespace hfgpu {{
 {body}
+}}  // namespace hfgpu
+"""
 
-#define HF_THIS_CLASS HF_CLASS_TRAITS({ci}, {bi}, {ki}, {A}{B}_{C}{D}, {nout}, {L})
-HF_THIS_CLASS
-#undef HF_THIS_CLASS
+CLASS_TU = """// GENERATED by gen_eri.py -- do not edit.
+// Kernels of quartet class ({A}{B}|{C}{D}): {roles} role(s).
+#include "../common.cuh"
+#include "{hdr}"
 
+namespace hfgpu {{
+{kernels}
+{traits}
 void register_class_{ci}(ClassKernels* k) {{
-    k->nd64 = k_nondiag<Cls_{A}{B}_{C}{D}, false>;
-    k->nd32 = k_nondiag<Cls_{A}{B}_{C}{D}, true>;
-{diag}    k->bi = {bi};
+{reg}    k->bi = {bi};
     k->ki = {ki};
     k->L = {L};
     k->nout = {nout};
@@ -422,26 +691,61 @@ def main(outdir: str):
     names = []
     flops = {}
     for ci, (bi, ki) in enumerate(class_list()):
-        g = ClassGen(PAIR_TYPES[bi], PAIR_TYPES[ki], "double")
-        g32 = ClassGen(PAIR_TYPES[bi], PAIR_TYPES[ki], "float", suffix="_f32")
-        body = g.emit() + "\n\n" + g32.emit()
-        diag = ""
-        if bi == ki:
-            diag = (f"    k->diag0 = k_diag<Cls_{g.A}{g.B}_{g.C}{g.D}, 0>;\n"
-                    f"    k->diag1 = k_diag<Cls_{g.A}{g.B}_{g.C}{g.D}, 1>;\n")
+        cuh, cu, info = class_source(ci, bi, ki)
+        flops[ci] = info
+        base = os.path.join(outdir, f"cls_{ci:02d}_{info['tag']}")
+        for ext, text in ((".cuh", cuh), (".cu", cu)):
+            if not os.path.exists(base + ext) or open(base + ext).read() != text:
+                with open(base + ext, "w") as fh:
+                    fh.write(text)
+        names.append(base + ".cu")
+    # host dispatch used by the host-compiled check of the generated code
+    lines = ["// GENERATED by gen_eri.py -- host dispatch of the class functions (tests only).", ""]
+    for ci, info in flops.items():
+        tag = info["tag"]
+        lines.append(f"inline void host_eri_{ci}(const GPair& b, const GPair& k, const GPrim* p, const double* t,")
+        lines.append(f"                          const float* tf, double* out, int f32) {{")
+        if info["roles"] == 1:
+            lines.append(f"    if (f32) {{ float o[{info['nout']}]; eri_{tag}_f32(b, k, p, tf, o);")
+            lines.append(f"        for (int i = 0; i < {info['nout']}; ++i) out[i] = o[i]; }}")
+            lines.append(f"    else eri_{tag}(b, k, p, t, out);")
         else:
-            diag = "    k->diag0 = nullptr;\n    k->diag1 = nullptr;\n"
-        flops[ci] = {"name": f"{g.A}{g.B}|{g.C}{g.D}", "L": g.L, "nout": g.nout,
-                     "flops_prim": g.flops_prim, "flops_quartet": g.flops_quartet,
-                     "vrr_terms": g.nvrr, "hrr_terms": g.nhrr}
-        text = CLASS_TU.format(A=g.A, B=g.B, C=g.C, D=g.D, body=body, ci=ci, bi=bi, ki=ki,
-                               nout=g.nout, L=g.L, diag=diag)
-        fn = os.path.join(outdir, f"cls_{ci:02d}_{g.A}{g.B}_{g.C}{g.D}.cu")
-        new = text
-        if not os.path.exists(fn) or open(fn).read() != new:
-            with open(fn, "w") as fh:
-                fh.write(new)
-        names.append(fn)
+            for r, outs in enumerate(info["role_outs"]):
+                n = len(outs)
+                idx = ", ".join(map(str, outs))
+                lines.append(f"    {{ static const int ix[{n}] = {{{idx}}}; double o[{n}]; float of[{n}];")
+                lines.append(f"      if (f32) {{ eri_{tag}_f32_r{r}(b, k, p, tf, of); for (int i = 0; i < {n}; ++i) o[i] = of[i]; }}")
+                lines.append(f"      else eri_{tag}_r{r}(b, k, p, t, o);")
+                lines.append(f"      for (int i = 0; i < {n}; ++i) out[ix[i]] = o[i]; }}")
+        lines.append("}")
+        lines.append(f"inline int host_scatter_{ci}(const double* e, double s, const GPair& b, const GPair& k,")
+        lines.append(f"                             const double* P, double* G, int nb, bool jonly) {{")
+        if info["roles"] == 1:
+            lines.append("    return 1;")
+        else:
+            for r, outs in enumerate(info["role_outs"]):
+                n = len(outs)
+                idx = ", ".join(map(str, outs))
+                lines.append(f"    {{ static const int ix[{n}] = {{{idx}}}; double o[{n}];")
+                lines.append(f"      for (int i = 0; i < {n}; ++i) o[i] = e[ix[i]];")
+                lines.append(f"      scat_{tag}_r{r}(o, s, b, k, P, G, nb, jonly); }}")
+            lines.append("    return 0;")
+        lines.append("}")
+    lines.append("typedef void (*HostEri)(const GPair&, const GPair&, const GPrim*, const double*, const float*, double*, int);")
+    lines.append("typedef int (*HostScat)(const double*, double, const GPair&, const GPair&, const double*, double*, int, bool);")
+    lines.append("static const HostEri HOST_ERI[] = {" + ", ".join(f"host_eri_{ci}" for ci in flops) + "};")
+    lines.append("static const HostScat HOST_SCAT[] = {" + ", ".join(f"host_scatter_{ci}" for ci in flops) + "};")
+    txt = "\n".join(lines) + "\n"
+    inc = "".join(f'#include "cls_{ci:02d}_{info["tag"]}.cuh"\n' for ci, info in flops.items())
+    inc += "namespace hfgpu {\n#include \"host_dispatch.inc\"\n}\n"
+    ai = os.path.join(outdir, "all_classes.inc")
+    if not os.path.exists(ai) or open(ai).read() != inc:
+        with open(ai, "w") as fh:
+            fh.write(inc)
+    hd = os.path.join(outdir, "host_dispatch.inc")
+    if not os.path.exists(hd) or open(hd).read() != txt:
+        with open(hd, "w") as fh:
+            fh.write(txt)
     import json
     fl = os.path.join(outdir, "class_flops.json")
     txt = json.dumps(flops, indent=1)

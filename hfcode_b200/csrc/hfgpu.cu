@@ -38,6 +38,7 @@
 
 #include "../../include/hfgpu.h"
 #include "common.cuh"
+#include "pairs.hpp"
 
 namespace hfgpu {
 #define HF_DECL_REG(ci) void register_class_##ci(ClassKernels* k);
@@ -63,7 +64,6 @@ thread_local std::string g_err;
     } while (0)
 
 constexpr double SHTHRESH = 1e-11;      // molprops.f90:163
-constexpr double EXTRATHRESH = 1e-12;   // precalc_kabs.f90:13
 
 // evaluate_maxdm.f90: one thread per unordered shell pair.
 __global__ void k_maxdm(const int* __restrict__ shtyp, const int* __restrict__ aosh, int nsh, int nb,
@@ -188,46 +188,6 @@ __global__ void k_symm(double* __restrict__ F, const double* __restrict__ G, int
 }
 
 // ------------------------------------------------------------- host ----
-struct HostPair {
-    GPair g;
-    int refcls;   // reference class index 0..9 (ss sp sd sl pp pd pl dd dl ll)
-    int refpos;   // position in the reference's class list
-};
-
-int ref_rank(int t) { return t == HFGPU_SHELL_S ? 0 : t == HFGPU_SHELL_P ? 1 : t == HFGPU_SHELL_D ? 2 : 3; }
-int nfunc_of(int t) { return t == HFGPU_SHELL_S ? 1 : t == HFGPU_SHELL_P ? 3 : t == HFGPU_SHELL_D ? 5 : 4; }
-
-// reference class (ss sp sd sl pp pd pl dd dl ll) of a rank pair (r1 <= r2)
-int ref_class(int r1, int r2) {
-    static const int tab[4][4] = {{0, 1, 2, 3}, {-1, 4, 5, 6}, {-1, -1, 7, 8}, {-1, -1, -1, 9}};
-    return tab[r1][r2];
-}
-// GPU pair type of a reference class, and whether the GPU pair swaps the
-// reference's (first, second) order; -1 for classes with pure p shells.
-int gpu_type_of_ref(int rc, bool* swap) {
-    switch (rc) {
-        case 0: *swap = false; return 0;  // ss -> SS
-        case 3: *swap = true; return 1;   // sl -> LS
-        case 9: *swap = false; return 2;  // ll -> LL
-        case 2: *swap = true; return 3;   // sd -> DS
-        case 8: *swap = false; return 4;  // dl -> DL
-        case 7: *swap = false; return 5;  // dd -> DD
-        default: *swap = false; return -1;
-    }
-}
-const int GPU_TO_REF[NPT] = {0, 3, 9, 2, 8, 7};
-
-long double boys_series(int m, long double T) {
-    // F_m(T) = e^-T sum_k (2T)^k / ((2m+1)(2m+3)...(2m+2k+1))
-    long double term = 1.0L / (2 * m + 1), sum = term;
-    for (int k = 1; k < 400; ++k) {
-        term *= 2.0L * T / (2 * m + 2 * k + 1);
-        sum += term;
-        if (term < sum * 1e-22L) break;
-    }
-    return expl(-T) * sum;
-}
-
 struct DevBuf {
     void* p = nullptr;
     size_t n = 0;
@@ -358,7 +318,8 @@ int launch_diag(hfgpu_handle* h, int mode, const double* P, double thr) {
         int n = (int)h->pairs[t].size();
         if (n == 0) continue;
         DiagArgs a{h->d_pairs[t], n, h->d_prims, h->d_boys, h->d_schw[t], h->d_md, h->nsh, P, h->d_G, h->nb, thr};
-        diag_kernel(t, mode)<<<(n + ND_THREADS - 1) / ND_THREADS, ND_THREADS, 0, h->stream>>>(a);
+        const ClassKernels& K = CLASS_KERNELS[class_index(t, t)];
+        diag_kernel(t, mode)<<<(n + K.dg_ppb - 1) / K.dg_ppb, K.dg_threads, 0, h->stream>>>(a);
         HF_CHECK(cudaGetLastError());
     }
     return HFGPU_OK;
@@ -369,8 +330,11 @@ int build_active(hfgpu_handle* h) {
     for (int t = 0; t < NPT; ++t) {
         int n = (int)h->pairs[t].size();
         h->schw[t].resize(n);
-        if (n) HF_CHECK(cudaMemcpy(h->schw[t].data(), h->d_schw[t], n * sizeof(double), cudaMemcpyDeviceToHost));
+        if (n)
+            HF_CHECK(cudaMemcpyAsync(h->schw[t].data(), h->d_schw[t], n * sizeof(double), cudaMemcpyDeviceToHost,
+                                     h->stream));
     }
+    HF_CHECK(cudaStreamSynchronize(h->stream));
     h->last_ref.assign(10, 0);
     long long total_q = 0;
     for (int t = 0; t < NPT; ++t) {
@@ -407,9 +371,12 @@ int build_active(hfgpu_handle* h) {
         }
         h->nact[t] = last;
         if (last) {
-            HF_CHECK(cudaMemcpy(h->d_apairs[t], ap.data(), last * sizeof(GPair), cudaMemcpyHostToDevice));
-            HF_CHECK(cudaMemcpy(h->d_ash[t], ash.data(), last * sizeof(int2), cudaMemcpyHostToDevice));
-            HF_CHECK(cudaMemcpy(h->d_aschw[t], asc.data(), last * sizeof(double), cudaMemcpyHostToDevice));
+            HF_CHECK(cudaMemcpyAsync(h->d_apairs[t], ap.data(), last * sizeof(GPair), cudaMemcpyHostToDevice,
+                                     h->stream));
+            HF_CHECK(cudaMemcpyAsync(h->d_ash[t], ash.data(), last * sizeof(int2), cudaMemcpyHostToDevice, h->stream));
+            HF_CHECK(cudaMemcpyAsync(h->d_aschw[t], asc.data(), last * sizeof(double), cudaMemcpyHostToDevice,
+                                     h->stream));
+            HF_CHECK(cudaStreamSynchronize(h->stream));
         }
     }
     // screening descriptors and quartet-list segments
@@ -433,7 +400,8 @@ int build_active(hfgpu_handle* h) {
     }
     h->ntot = start;
     total_q = qoff;
-    HF_CHECK(cudaMemcpy(h->d_cls, h->hcls, sizeof(h->hcls), cudaMemcpyHostToDevice));
+    HF_CHECK(cudaMemcpyAsync(h->d_cls, h->hcls, sizeof(h->hcls), cudaMemcpyHostToDevice, h->stream));
+    HF_CHECK(cudaStreamSynchronize(h->stream));
     if ((size_t)total_q > h->qcap) {
         if (h->d_q) cudaFree(h->d_q);
         h->d_q = nullptr;
@@ -472,9 +440,9 @@ int run_non_diag(hfgpu_handle* h, const double* P, double thr, int jonly, double
             if (n == 0) continue;
             NDArgs a{h->d_q + h->hcls[c].qoff, (int)n, prec, h->hcls[c].cap, h->d_apairs[K.bi], h->d_apairs[K.ki],
                      h->d_prims, h->d_boys, h->d_boysf, P, h->d_G, h->nb, thr, jonly, h->d_stats + c};
-            long long blocks = (n + ND_THREADS - 1) / ND_THREADS;
+            long long blocks = (n + K.nd_qpb - 1) / K.nd_qpb;
             if (h->timing) HF_CHECK(cudaEventRecord(h->ev[2 * c], h->stream));
-            (prec ? K.nd32 : K.nd64)<<<(int)blocks, ND_THREADS, 0, h->stream>>>(a);
+            (prec ? K.nd32 : K.nd64)<<<(int)blocks, K.nd_threads, 0, h->stream>>>(a);
             HF_CHECK(cudaGetLastError());
             if (h->timing) {
                 HF_CHECK(cudaEventRecord(h->ev[2 * c + 1], h->stream));
@@ -513,8 +481,6 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
     h->nzet.assign(B->nzet, B->nzet + B->nsh);
     h->aosh.assign(B->aosh, B->aosh + B->nsh);
     const int MP = B->maxprim;
-    const double PI = 3.141592653589793238462643383279502884197;
-    const double RT2PI54 = std::sqrt(2.0 * PI * PI * std::sqrt(PI));
     for (int s = 0; s < h->nsh; ++s) {
         int t = h->shtyp[s];
         if (t != HFGPU_SHELL_S && t != HFGPU_SHELL_D && t != HFGPU_SHELL_L) {
@@ -526,66 +492,13 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
             return set_err(HFGPU_ERR_ARG, "hfgpu_init: bad primitive count");
         }
     }
-    // pair lists in the reference's enumeration order (precalc_kabs.f90:38-90)
     std::vector<GPrim> prims;
-    h->refcount.assign(10, 0);
-    for (int s1 = 0; s1 < h->nsh; ++s1)
-        for (int s2 = 0; s2 <= s1; ++s2) {
-            int r1 = s1, r2 = s2;
-            if (ref_rank(h->shtyp[r1]) > ref_rank(h->shtyp[r2])) std::swap(r1, r2);
-            int rc = ref_class(ref_rank(h->shtyp[r1]), ref_rank(h->shtyp[r2]));
-            bool swp = false;
-            int gt = gpu_type_of_ref(rc, &swp);
-            int a = swp ? r2 : r1, b = swp ? r1 : r2;
-            HostPair hp;
-            hp.refcls = rc;
-            hp.refpos = h->refcount[rc]++;
-            GPair& g = hp.g;
-            for (int x = 0; x < 3; ++x) {
-                g.A[x] = B->xsh[3 * a + x];
-                g.B[x] = B->xsh[3 * b + x];
-            }
-            g.sa = a;
-            g.sb = b;
-            g.aoa = B->aosh[a];
-            g.aob = B->aosh[b];
-            g.p0 = (int)prims.size();
-            double r2ab = 0;
-            for (int x = 0; x < 3; ++x) r2ab += (g.A[x] - g.B[x]) * (g.A[x] - g.B[x]);
-            for (int za = 0; za < h->nzet[a]; ++za)
-                for (int zb = 0; zb < h->nzet[b]; ++zb) {
-                    double ea = B->zeta[(size_t)a * MP + za], eb = B->zeta[(size_t)b * MP + zb];
-                    double p = ea + eb, pm1 = 1.0 / p, q = ea * eb * pm1;
-                    double K = RT2PI54 * std::exp(-q * r2ab) * pm1 * B->djk[(size_t)a * MP + za] *
-                               B->djk[(size_t)b * MP + zb];
-                    if (std::fabs(K) * std::sqrt(pm1) < EXTRATHRESH) continue;  // negab
-                    GPrim gp;
-                    gp.p = p;
-                    for (int x = 0; x < 3; ++x) gp.P[x] = (ea * g.A[x] + eb * g.B[x]) * pm1;
-                    gp.K = K;
-                    gp.w1 = h->shtyp[a] == HFGPU_SHELL_L ? B->djkl[(size_t)a * MP + za] : 1.0;
-                    gp.w2 = h->shtyp[b] == HFGPU_SHELL_L ? B->djkl[(size_t)b * MP + zb] : 1.0;
-                    gp.pad = 0.0;
-                    prims.push_back(gp);
-                }
-            g.np = (int)prims.size() - g.p0;
-            h->pairs[gt].push_back(hp);
-            h->npairs++;
-        }
-    // Boys tables: c_k = F_{M+k}(T_j) (-1)^k / k!, M = 0..8, T_j = j/8
-    std::vector<double> bt((size_t)(BOYS_MMAX + 1) * BOYS_NPT * BOYS_K);
-    std::vector<float> btf(bt.size());
-    for (int M = 0; M <= BOYS_MMAX; ++M)
-        for (int j = 0; j < BOYS_NPT; ++j) {
-            long double T = j / 8.0L, fact = 1.0L;
-            for (int k = 0; k < BOYS_K; ++k) {
-                if (k) fact *= k;
-                long double v = boys_series(M + k, T) / fact * ((k & 1) ? -1.0L : 1.0L);
-                size_t i = ((size_t)M * BOYS_NPT + j) * BOYS_K + k;
-                bt[i] = (double)v;
-                btf[i] = (float)v;
-            }
-        }
+    std::vector<HostPair> plist[NPT];
+    h->npairs = build_pairs(B, plist, prims, h->refcount);
+    for (int t = 0; t < NPT; ++t) h->pairs[t] = std::move(plist[t]);
+    std::vector<double> bt;
+    std::vector<float> btf;
+    build_boys_table(bt, btf);
     cudaError_t ce = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (ce != cudaSuccess) {
         std::string m = std::string("cudaStreamCreate: ") + cudaGetErrorString(ce);
@@ -635,6 +548,12 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
     }
     if (ce != cudaSuccess) {
         std::string m = std::string("hfgpu_init upload: ") + cudaGetErrorString(ce);
+        hfgpu_finalize(h);
+        return set_err(HFGPU_ERR_CUDA, m);
+    }
+    ce = cudaDeviceSynchronize();
+    if (ce != cudaSuccess) {
+        std::string m = std::string("hfgpu_init: ") + cudaGetErrorString(ce);
         hfgpu_finalize(h);
         return set_err(HFGPU_ERR_CUDA, m);
     }
