@@ -31,6 +31,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <type_traits>
@@ -298,26 +299,28 @@ int download_f(hfgpu_handle* h, double* f) {
     return HFGPU_OK;
 }
 
-int launch_maxdm(hfgpu_handle* h, const double* P) {
+int launch_maxdm(hfgpu_handle* h, const double* P, double* md = nullptr) {
     long long np = (long long)h->nsh * (h->nsh + 1) / 2;
     int blocks = (int)((np + 255) / 256);
-    k_maxdm<<<blocks, 256, 0, h->stream>>>(h->d_shtyp, h->d_aosh, h->nsh, h->nb, P, h->d_md);
+    k_maxdm<<<blocks, 256, 0, h->stream>>>(h->d_shtyp, h->d_aosh, h->nsh, h->nb, P, md ? md : h->d_md);
     HF_CHECK(cudaGetLastError());
     return HFGPU_OK;
 }
 
-int launch_symm(hfgpu_handle* h, double* F) {
+int launch_symm(hfgpu_handle* h, double* F, const double* G = nullptr) {
     long long n = (long long)h->nb * h->nb;
-    k_symm<<<(int)((n + 255) / 256), 256, 0, h->stream>>>(F, h->d_G, h->nb);
+    k_symm<<<(int)((n + 255) / 256), 256, 0, h->stream>>>(F, G ? G : h->d_G, h->nb);
     HF_CHECK(cudaGetLastError());
     return HFGPU_OK;
 }
 
-int launch_diag(hfgpu_handle* h, int mode, const double* P, double thr) {
+int launch_diag(hfgpu_handle* h, int mode, const double* P, double thr, double* G = nullptr,
+                const double* md = nullptr) {
     for (int t = 0; t < NPT; ++t) {
         int n = (int)h->pairs[t].size();
         if (n == 0) continue;
-        DiagArgs a{h->d_pairs[t], n, h->d_prims, h->d_boys, h->d_schw[t], h->d_md, h->nsh, P, h->d_G, h->nb, thr};
+        DiagArgs a{h->d_pairs[t], n, h->d_prims, h->d_boys, h->d_schw[t], md ? md : h->d_md, h->nsh, P,
+                   G ? G : h->d_G, h->nb, thr};
         const ClassKernels& K = CLASS_KERNELS[class_index(t, t)];
         diag_kernel(t, mode)<<<(n + K.dg_ppb - 1) / K.dg_ppb, K.dg_threads, 0, h->stream>>>(a);
         HF_CHECK(cudaGetLastError());
@@ -726,3 +729,63 @@ int hfgpu_measure_fma_peak(double* fp64_gflops, double* fp32_gflops) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------ no-allocation variant ----
+// Scratch of hfgpu_fock_build_diag_static: the one-triangle accumulation
+// buffer G (nb x nb) and the shell-pair density maxima (nsh x nsh) live in
+// this file-scope device array instead of memory from cudaMalloc.  Every GPU
+// that loads the library holds it (10.1 MB) until the process exits.
+namespace {
+constexpr int STATIC_MAX_NB = 1024;
+constexpr int STATIC_MAX_NSH = 512;
+constexpr size_t STATIC_SCRATCH_DOUBLES =
+    (size_t)STATIC_MAX_NB * STATIC_MAX_NB + (size_t)STATIC_MAX_NSH * STATIC_MAX_NSH;
+}  // namespace
+
+static __device__ __align__(256) double g_static_scratch[STATIC_SCRATCH_DOUBLES];
+
+namespace {
+constexpr int STATIC_MAX_DEVICES = 64;
+std::mutex g_static_mu;
+double* g_static_ptr[STATIC_MAX_DEVICES] = {};
+
+// Device address of g_static_scratch on the current device.  Host code sees
+// only a host-side stand-in under that name, so the address is looked up once
+// per device, with that device current, and cached.
+int static_scratch(double** out) {
+    int dev = 0;
+    HF_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= STATIC_MAX_DEVICES) return set_err(HFGPU_ERR_UNSUPPORTED, "device index out of range");
+    std::lock_guard<std::mutex> lk(g_static_mu);
+    if (!g_static_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess || !p)
+            return set_err(HFGPU_ERR_CUDA, std::string("cudaGetSymbolAddress(g_static_scratch): ") +
+                                               cudaGetErrorString(e));
+        g_static_ptr[dev] = (double*)p;
+    }
+    *out = g_static_ptr[dev];
+    return HFGPU_OK;
+}
+}  // namespace
+
+extern "C" int hfgpu_fock_build_diag_static(hfgpu_handle* h, double* f_dev, const double* p_dev, double thr) {
+    if (!h || !f_dev || !p_dev) return set_err(HFGPU_ERR_ARG, "null argument");
+    if (h->nb > STATIC_MAX_NB || h->nsh > STATIC_MAX_NSH)
+        return set_err(HFGPU_ERR_ARG, "hfgpu_fock_build_diag_static: nb " + std::to_string(h->nb) + " / nsh " +
+                                          std::to_string(h->nsh) + " exceeds the static scratch limit of nb <= " +
+                                          std::to_string(STATIC_MAX_NB) + ", nsh <= " +
+                                          std::to_string(STATIC_MAX_NSH));
+    if (!h->have_schwarz) return set_err(HFGPU_ERR_STATE, "fock_build_initial_diag has not been called");
+    double* scratch = nullptr;
+    int rc = static_scratch(&scratch);
+    if (rc) return rc;
+    double* G = scratch;
+    double* md = scratch + (size_t)STATIC_MAX_NB * STATIC_MAX_NB;
+    // G keeps the previous call's sums: clear it first
+    HF_CHECK(cudaMemsetAsync(G, 0, (size_t)h->nb * h->nb * sizeof(double), h->stream));
+    if ((rc = launch_maxdm(h, p_dev, md))) return rc;
+    if ((rc = launch_diag(h, 1, p_dev, thr, G, md))) return rc;
+    return launch_symm(h, f_dev, G);
+}

@@ -59,6 +59,7 @@ def _load():
     lib.hfgpu_finalize.argtypes = [vp]
     lib.hfgpu_last_error.restype = ctypes.c_char_p
     lib.hfgpu_measure_fma_peak.argtypes = [d, d]
+    lib.hfgpu_fock_build_diag_static.argtypes = [vp, vp, vp, ctypes.c_double]
     return lib
 
 
@@ -68,7 +69,8 @@ EXPORTS = ["hfgpu_init", "hfgpu_fock_build_initial_diag", "hfgpu_fock_build_diag
            "hfgpu_fock_build_non_diag", "hfgpu_fock_build_non_diag_j_only",
            "hfgpu_fock_build_non_diag_mixed", "hfgpu_fock_build_device", "hfgpu_dims",
            "hfgpu_get_schwarz", "hfgpu_get_class_stats", "hfgpu_set_timing", "hfgpu_stream",
-           "hfgpu_finalize", "hfgpu_last_error", "hfgpu_measure_fma_peak"]
+           "hfgpu_finalize", "hfgpu_last_error", "hfgpu_measure_fma_peak",
+           "hfgpu_fock_build_diag_static", "hfgpu_one_electron"]
 
 
 def measure_fma_peak():
@@ -152,6 +154,12 @@ class FockBuilder:
         _check(_lib.hfgpu_fock_build_device(self.h, ctypes.c_void_p(f_ptr), ctypes.c_void_p(p_ptr),
                                             float(thr_diag), float(thr_non_diag), float(fp32_cutoff)),
                "fock_build_device")
+
+    def fock_build_diag_static(self, f_ptr: int, p_ptr: int, thr: float):
+        """fock_build_diag on device pointers using the library's static
+        scratch (no device allocation; see include/hfgpu.h)."""
+        _check(_lib.hfgpu_fock_build_diag_static(self.h, ctypes.c_void_p(f_ptr), ctypes.c_void_p(p_ptr),
+                                                 float(thr)), "fock_build_diag_static")
 
     def stream(self) -> int:
         return int(_lib.hfgpu_stream(self.h) or 0)

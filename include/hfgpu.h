@@ -115,6 +115,21 @@ int hfgpu_measure_fma_peak(double* fp64_gflops, double* fp32_gflops);
 int hfgpu_one_electron(const hfgpu_basis* basis, int natom, const double* charges, const double* xyz,
                        double* S, double* T, double* V);
 
+/* fock_build_diag on device pointers for callers that cannot allocate GPU
+ * memory at the call site -- for example code that runs where cudaMalloc is
+ * not allowed, or that must not grow the device footprint after start-up.
+ * No counterpart in the reference.  It allocates nothing: its scratch (the
+ * accumulation buffer and the shell-pair density maxima) is a file-scope
+ * __device__ array of 10.1 MB that every GPU loading the library holds until
+ * exit, so nb <= 1024 and nsh <= 512 (larger sizes return HFGPU_ERR_ARG).
+ * f_dev += G_diag(p_dev), enqueued on the handle's stream.  The handle must
+ * come from hfgpu_init + hfgpu_fock_build_initial_diag, called earlier where
+ * allocation is allowed.  The first call on a device looks up the scratch
+ * address for that device; make that first call before any stream capture.
+ * All calls share the one scratch array, so calls that overlap on the GPU
+ * (other streams, other threads, other handles) race; serialise them. */
+int hfgpu_fock_build_diag_static(hfgpu_handle* h, double* f_dev, const double* p_dev, double thr);
+
 /* Releases all device memory of the handle (dealloc_integs.f90's role). */
 int hfgpu_finalize(hfgpu_handle* h);
 
