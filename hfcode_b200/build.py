@@ -51,6 +51,7 @@ def build(jobs: int = 0, verbose: bool = True) -> str:
     gen_srcs = gen_eri.main(os.path.join(CSRC, "generated"))
     os.makedirs(BUILD, exist_ok=True)
     common = [os.path.join(CSRC, "common.cuh"), os.path.join(CSRC, "types.cuh"), os.path.join(CSRC, "pairs.hpp"),
+              os.path.join(CSRC, "scatter.cuh"),
               os.path.join(HERE, "..", "include", "hfgpu.h"),
               os.path.join(HERE, "..", "include", "hfgpu_basis.h")]
     srcs = [os.path.join(CSRC, "hfgpu.cu"), os.path.join(CSRC, "onee.cpp")] + sorted(gen_srcs)

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include "types.cuh"
+#include "scatter.cuh"
 
 #include <cstdint>
 #include <type_traits>
@@ -274,15 +275,78 @@ __global__ void __launch_bounds__(ND_THREADS) k_diag(DiagArgs a) {
 }
 
 
+// Arguments of the staged classes' kernels: a chunk of the class's quartet
+// list, and the scratch it goes through (accumulators, outputs and the
+// per-role maxima, each [row][stride] with one column per quartet).
+struct StagedArgs {
+    const uint2* quartets;
+    int n;                 // quartets in this chunk
+    long long q0;          // chunk start within the list
+    int from_back;         // FP32 entries fill the list from the back
+    long long cap;
+    const GPair* bra;
+    const GPair* ket;
+    const GPrim* prims;
+    const double* boys;
+    const float* boysf;
+    double* acc;
+    double* out;
+    double* mx;
+    size_t stride;         // columns of the scratch rows (chunk capacity)
+    int nroles;            // rows of mx
+    const double* P;
+    double* G;
+    int nb;
+    double thr;
+    int jonly;
+    int f32;
+    ClassStats* stats;
+};
+
+__device__ __forceinline__ uint2 staged_quartet(const StagedArgs& a, int t) {
+    const long long i = a.q0 + t;
+    return a.from_back ? a.quartets[a.cap - 1 - i] : a.quartets[i];
+}
+
+// Post-screen (max |e| over all roles < thr, fock_build_non_diag.f90:69) and
+// J/K scatter of a staged chunk, one thread per quartet.
+template <int NA, int NB, int NC, int ND>
+__global__ void __launch_bounds__(ND_THREADS) k_scatter_staged(StagedArgs a) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long nsc = 0, npr = 0;
+    if (t < a.n) {
+        double m = 0.0;
+        for (int r = 0; r < a.nroles; ++r) m = fmax(m, a.mx[(size_t)r * a.stride + t]);
+        const uint2 q = staged_quartet(a, t);
+        const GPair bra = a.bra[q.x];
+        const GPair ket = a.ket[q.y];
+        npr = (unsigned long long)(bra.np * ket.np);
+        if (!(m < a.thr)) {
+            nsc = 1;
+            const double s = (bra.sa == bra.sb ? 0.5 : 1.0) * (ket.sa == ket.sb ? 0.5 : 1.0);
+            scatter_strided<NA, NB, NC, ND>(a.out + t, a.stride, s, bra, ket, a.P, a.G, a.nb, a.jonly != 0);
+        }
+    }
+    if (a.stats) warp_add_stats(a.stats, nsc, npr, a.f32 ? nsc : 0ull);
+}
+
 typedef void (*NDKernel)(NDArgs);
 typedef void (*DiagKernel)(DiagArgs);
+typedef void (*StagedKernel)(StagedArgs);
+constexpr int MAXR = 64;
 
 // Kernels of one quartet class, filled by the class's translation unit.
+// mode 0: direct (nd64/nd32); 1: staged output roles (sb*); 2: staged
+// accumulator roles (sa*) then output roles (sb*).  All staged classes end
+// with scat.
 struct ClassKernels {
+    int mode;
     NDKernel nd64, nd32;
     DiagKernel diag0, diag1;  // only for classes (X|X)
     int nd_threads, nd_qpb;   // block size and quartets per block
     int dg_threads, dg_ppb;   // block size and pairs per block (diag)
+    int nacc, nrole_a, nrole_b;
+    StagedKernel sa64[MAXR], sa32[MAXR], sb64[MAXR], sb32[MAXR], scat;
     int bi, ki, L, nout;
 };
 

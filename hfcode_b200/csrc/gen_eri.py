@@ -282,17 +282,14 @@ class ClassGen:
         return groups
 
     # ---------------------------------------------------------------- emit
-    def emit_role(self, fname: str, outs: List[int]):
-        """Device function computing the outputs `outs` (flat indices) into
-        out[0..len(outs)).  Returns (code, stats)."""
+    def _vrr_block(self, keys):
+        """Primitive loops: Boys, VRR and the weighted accumulation of the
+        accumulator keys.  Returns (lines, acc name map, stats)."""
         ft = self.ft
         dbl = ft == "double"
         L = self.L
         cv = (lambda s: s) if dbl else (lambda s: f"(float)({s})")
-        needed_acc = set()
-        for n in outs:
-            needed_acc |= self.out_leaves(self.outputs[n])
-        targets = sorted({(e, f) for (_, _, e, f) in needed_acc})
+        targets = sorted({(e, f) for (_, _, e, f) in keys})
 
         def gen_vrr(order):
             em = Emitter(ft)
@@ -305,16 +302,11 @@ class ClassGen:
         em_k, v_k = gen_vrr("ket")
         em, vrr = (em_b, v_b) if v_b.nops <= v_k.nops else (em_k, v_k)
         acc = {}
-        for key in sorted(needed_acc, key=lambda k: (k[0], k[1], sum(k[2]), k[2], sum(k[3]), k[3])):
+        for key in sorted(keys, key=lambda k: (k[0], k[1], sum(k[2]), k[2], sum(k[3]), k[3])):
             bi, ki, e, f = key
             acc[key] = f"a{bi}{ki}_{''.join(map(str, e))}_{''.join(map(str, f))}"
         out = []
         w = out.append
-        w(f"// ({self.A}{self.B}|{self.C}{self.D}) outputs {outs[0]}..{outs[-1]} ({len(outs)}): L={L}, "
-          f"{len(acc)} accumulators, VRR {vrr.nops} terms ({vrr.order}-first)")
-        w(f"__device__ __forceinline__ void {fname}(const GPair& bra, const GPair& ket,")
-        w(f"    const GPrim* __restrict__ prims, const {ft}* __restrict__ btab, {ft}* __restrict__ out)")
-        w("{")
         w(f"    {ft} " + ", ".join(f"{n} = 0" for n in acc.values()) + ";")
         w("    const double Ax = bra.A[0], Ay = bra.A[1], Az = bra.A[2];")
         w("    const double Cx = ket.A[0], Cy = ket.A[1], Cz = ket.A[2];")
@@ -379,10 +371,18 @@ class ClassGen:
             w(f"            {nm} += {' * '.join(wexp + [src])};")
         w("        }")
         w("    }")
-        w(f"    const {ft} AB0 = {cv('bra.A[0] - bra.B[0]')}, AB1 = {cv('bra.A[1] - bra.B[1]')}, "
-          f"AB2 = {cv('bra.A[2] - bra.B[2]')};")
-        w(f"    const {ft} CD0 = {cv('ket.A[0] - ket.B[0]')}, CD1 = {cv('ket.A[1] - ket.B[1]')}, "
-          f"CD2 = {cv('ket.A[2] - ket.B[2]')};")
+        nbracket = sum(line.count(" - r") for line in em.lines)
+        return out, acc, {"vrr": vrr.nops, "bracket": nbracket, "acc": len(acc), "order": vrr.order}
+
+    def _hrr_block(self, outs, leaf, ft):
+        """HRR on ket and bra plus the spherical transform for `outs`;
+        leaf(key) names the contracted accumulator.  Returns (lines, value
+        expressions per output, stats)."""
+        cv = (lambda s: s) if ft == "double" else (lambda s: f"(float)({s})")
+        lines = [f"    const {ft} AB0 = {cv('bra.A[0] - bra.B[0]')}, AB1 = {cv('bra.A[1] - bra.B[1]')}, "
+                 f"AB2 = {cv('bra.A[2] - bra.B[2]')};",
+                 f"    const {ft} CD0 = {cv('ket.A[0] - ket.B[0]')}, CD1 = {cv('ket.A[1] - ket.B[1]')}, "
+                 f"CD2 = {cv('ket.A[2] - ket.B[2]')};"]
         hem = Emitter(ft)
         memo = {}
 
@@ -391,7 +391,7 @@ class ClassGen:
             if key in memo:
                 return memo[key]
             if d == Z3:
-                r = acc[(bi, ki, e, c)]
+                r = leaf((bi, ki, e, c))
             else:
                 i = max(range(3), key=lambda k: (d[k], -k))
                 d1 = add(d, i, -1)
@@ -416,27 +416,87 @@ class ClassGen:
             memo[key] = r
             return r
 
-        def cart_val(c4):
-            bi, ki = self.combo_of(c4)
-            a, b, c, d = (self.cl[ax][c4[ax]][1] for ax in range(4))
-            return bra_hrr(bi, ki, a, b, c, d)
-
-        sph = []
+        vals = []
         nsph = 0
-        for r, n in enumerate(outs):
+        for n in outs:
             terms = []
             for coef, c4 in self.cart_terms(self.outputs[n]):
-                v = cart_val(c4)
+                bi, ki = self.combo_of(c4)
+                a, b, c, d = (self.cl[ax][c4[ax]][1] for ax in range(4))
+                v = bra_hrr(bi, ki, a, b, c, d)
                 terms.append(v if coef == 1.0 else f"{fmt_coef(coef, ft)}*{v}")
             nsph += len(terms) - 1
-            sph.append(f"    out[{r}] = {' + '.join(terms)};")
-        for line in hem.lines:
-            w(line)
-        out.extend(sph)
-        w("}")
-        nbracket = sum(line.count(" - r") for line in em.lines)
-        stats = {"vrr": vrr.nops, "bracket": nbracket, "acc": len(acc), "hrr": len(hem.lines), "sph": nsph}
-        return "\n".join(out), stats
+            vals.append(" + ".join(terms))
+        lines += hem.lines
+        return lines, vals, {"hrr": len(hem.lines), "sph": nsph}
+
+    def needed_keys(self, outs):
+        keys = set()
+        for n in outs:
+            keys |= self.out_leaves(self.outputs[n])
+        return keys
+
+    def all_keys(self):
+        return self.needed_keys(range(self.nout))
+
+    def emit_role(self, fname: str, outs: List[int]):
+        """Device function computing the outputs `outs` (flat indices) into
+        out[0..len(outs)).  Returns (code, stats)."""
+        ft = self.ft
+        vlines, acc, vst = self._vrr_block(self.needed_keys(outs))
+        hlines, vals, hst = self._hrr_block(outs, lambda k: acc[k], ft)
+        out = [f"// ({self.A}{self.B}|{self.C}{self.D}) outputs {outs[0]}..{outs[-1]} ({len(outs)}): L={self.L}, "
+               f"{vst['acc']} accumulators, VRR {vst['vrr']} terms ({vst['order']}-first)",
+               f"__device__ __forceinline__ void {fname}(const GPair& bra, const GPair& ket,",
+               f"    const GPrim* __restrict__ prims, const {ft}* __restrict__ btab, {ft}* __restrict__ out)",
+               "{"]
+        out += vlines + hlines
+        out += [f"    out[{r}] = {v};" for r, v in enumerate(vals)]
+        out.append("}")
+        return "\n".join(out), {**vst, **hst}
+
+    def emit_acc_role(self, fname: str, keys: List[Tuple]):
+        """Stage-A device function: the contracted accumulators `keys`,
+        written to dst[k * stride] (k = position in `keys`)."""
+        ft = self.ft
+        vlines, acc, vst = self._vrr_block(set(keys))
+        out = [f"// ({self.A}{self.B}|{self.C}{self.D}) accumulators ({len(keys)}): VRR {vst['vrr']} terms "
+               f"({vst['order']}-first)",
+               f"__device__ __forceinline__ void {fname}(const GPair& bra, const GPair& ket,",
+               f"    const GPrim* __restrict__ prims, const {ft}* __restrict__ btab, double* __restrict__ dst, "
+               f"size_t stride)",
+               "{"]
+        out += vlines
+        out += [f"    dst[{k} * stride] = (double){acc[key]};" for k, key in enumerate(keys)]
+        out.append("}")
+        return "\n".join(out), vst
+
+    def emit_hrr_role(self, fname: str, outs: List[int], keyidx: Dict[Tuple, int]):
+        """Stage-B device function: outputs `outs` from the accumulators in
+        src[keyidx[key] * stride], written to dst[r * stride]; returns
+        max |value|."""
+        loaded = {}
+        lines = []
+
+        def leaf(key):
+            if key not in loaded:
+                nm = f"L{keyidx[key]}"
+                loaded[key] = nm
+                lines.append(f"    const double {nm} = __ldg(src + {keyidx[key]} * stride);")
+            return loaded[key]
+
+        hlines, vals, hst = self._hrr_block(outs, leaf, "double")
+        out = [f"// ({self.A}{self.B}|{self.C}{self.D}) outputs {outs[0]}..{outs[-1]} ({len(outs)}) from accumulators",
+               f"__device__ __forceinline__ double {fname}(const GPair& bra, const GPair& ket,",
+               f"    const double* __restrict__ src, double* __restrict__ dst, size_t stride)",
+               "{"]
+        out += hlines[:2] + lines + hlines[2:]
+        out.append("    double mx = 0.0;")
+        for r, v in enumerate(vals):
+            out.append(f"    {{ const double v = {v}; dst[{r} * stride] = v; mx = fmax(mx, fabs(v)); }}")
+        out.append("    return mx;")
+        out.append("}")
+        return "\n".join(out), hst
 
     def flop_model(self):
         """Algorithmic FLOPs of the class in its single-function formulation
@@ -494,120 +554,197 @@ class ClassGen:
         return "\n".join(lines)
 
 
-ACC_MAX = 96
-OUT_MAX = 48
-MAX_ROLES = 10
+ACC_MAX = 64        # accumulators per output role (register budget)
+OUT_MAX = 32        # outputs per output role
+MAX_ROLES2 = 12     # beyond this, the class goes through the accumulator stage
+ACC_GROUP = 48      # accumulators per stage-A role (d-heavy classes)
+OUT_GROUP3 = 25     # outputs per stage-B role (d-heavy classes)
+MAXR = 64           # role slots in ClassKernels
+
+
+def acc_groups(g: "ClassGen"):
+    """Partition of all accumulator keys into stage-A roles; the key order
+    that minimises the summed VRR terms wins."""
+    keys = list(g.all_keys())
+    orders = {
+        "ket": lambda k: (k[1], sum(k[3]), k[3], k[0], sum(k[2]), k[2]),
+        "bra": lambda k: (k[0], sum(k[2]), k[2], k[1], sum(k[3]), k[3]),
+        "f": lambda k: (sum(k[3]), k[3], k[1], k[0], sum(k[2]), k[2]),
+        "e": lambda k: (sum(k[2]), k[2], k[0], k[1], sum(k[3]), k[3]),
+    }
+    best = None
+    for name, fn in orders.items():
+        ks = sorted(keys, key=fn)
+        groups = [ks[i:i + ACC_GROUP] for i in range(0, len(ks), ACC_GROUP)]
+        cost = sum(g._vrr_block(set(gr))[2]["vrr"] for gr in groups)
+        if best is None or cost < best[0]:
+            best = (cost, groups)
+    return best[1]
 
 
 def class_source(ci: int, bi: int, ki: int):
     """Header (device functions) and translation unit (kernels) of one
-    quartet class; returns (cuh_text, cu_text, info)."""
+    quartet class; returns (cuh_text, cu_text, info).
+
+    Three shapes:
+      direct  one thread per quartet computes the whole block (k_nondiag);
+      staged2 the outputs are split into roles, one kernel launch per role
+              (uniform code per launch), each writing its outputs and their
+              max to a scratch buffer; k_scatter_staged applies the
+              post-screen and the J/K scatter;
+      staged3 (d-heavy) stage-A roles write the contracted [e0|f0]
+              accumulators to scratch, stage-B roles apply the HRR and the
+              spherical transform to slices of the outputs, then the same
+              scatter kernel."""
     g = ClassGen(PAIR_TYPES[bi], PAIR_TYPES[ki], "double")
+    g32 = ClassGen(PAIR_TYPES[bi], PAIR_TYPES[ki], "float", suffix="_f32")
     g.flop_model()
     roles = g.partition(ACC_MAX, OUT_MAX)
-    if len(roles) > MAX_ROLES:  # d-heavy classes: one thread per quartet
-        roles = [list(range(g.nout))]
-    R = len(roles)
-    g32 = ClassGen(PAIR_TYPES[bi], PAIR_TYPES[ki], "float", suffix="_f32")
-    funcs = []
-    if R == 1:
+    funcs, kern = [], []
+    reg = []
+    NA, NB, NC, ND = g.nf
+    info = {"name": f"{g.A}{g.B}|{g.C}{g.D}", "tag": g.tag, "L": g.L, "nout": g.nout,
+            "flops_prim": g.flops_prim, "flops_quartet": g.flops_quartet,
+            "vrr_terms": g.nvrr, "hrr_terms": g.nhrr}
+    if len(roles) == 1:
+        mode = "direct"
         code, _ = g.emit_role(g.name, roles[0])
         code32, _ = g32.emit_role(g32.name, roles[0])
         funcs += [code, code32]
-    else:
+        reg.append(f"    k->mode = 0;")
+        reg.append(f"    k->nd64 = k_nondiag<Cls_{g.tag}, false>;")
+        reg.append(f"    k->nd32 = k_nondiag<Cls_{g.tag}, true>;")
+        reg.append(f"    k->nd_threads = ND_THREADS;\n    k->nd_qpb = ND_THREADS;")
+        if bi == ki:
+            reg.append(f"    k->diag0 = k_diag<Cls_{g.tag}, 0>;\n    k->diag1 = k_diag<Cls_{g.tag}, 1>;")
+            reg.append(f"    k->dg_threads = ND_THREADS;\n    k->dg_ppb = ND_THREADS;")
+        info.update(roles=1, role_sizes=[g.nout], role_outs=[roles[0]], acc_groups=[])
+    elif len(roles) <= MAX_ROLES2:
+        mode = "staged2"
         for r, outs in enumerate(roles):
             code, _ = g.emit_role(f"{g.name}_r{r}", outs)
             code32, _ = g32.emit_role(f"{g32.name}_r{r}", outs)
-            funcs += [code, code32, g.emit_scatter(f"scat_{g.tag}_r{r}", outs)]
-    cuh = CLASS_CUH.format(A=g.A, B=g.B, C=g.C, D=g.D, roles=R, body="\n\n".join(funcs))
-    info = {"name": f"{g.A}{g.B}|{g.C}{g.D}", "tag": g.tag, "L": g.L, "nout": g.nout, "roles": R,
-            "role_sizes": [len(x) for x in roles], "role_outs": roles,
-            "flops_prim": g.flops_prim, "flops_quartet": g.flops_quartet,
-            "vrr_terms": g.nvrr, "hrr_terms": g.nhrr}
-    if R == 1:
-        reg = (f"    k->nd64 = k_nondiag<Cls_{g.tag}, false>;\n"
-               f"    k->nd32 = k_nondiag<Cls_{g.tag}, true>;\n"
-               f"    k->nd_threads = ND_THREADS;\n    k->nd_qpb = ND_THREADS;\n")
+            funcs += [code, code32]
+            stores = "\n".join(f"    {{ const double v = (double)e[{i}]; a.out[(size_t){n} * a.stride + t] = v; "
+                               f"mx = fmax(mx, fabs(v)); }}" for i, n in enumerate(outs))
+            kern.append(f"""
+template <bool F32>
+__global__ void __launch_bounds__(ND_THREADS, 3) k_s2_{g.tag}_r{r}(StagedArgs a) {{
+    using Real = typename std::conditional<F32, float, double>::type;
+    __shared__ Real sboys[BOYS_NPT * BOYS_K];
+    if constexpr (F32) stage_boys<{g.L}>(sboys, a.boysf);
+    else stage_boys<{g.L}>(sboys, a.boys);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.n) return;
+    const uint2 q = staged_quartet(a, t);
+    const GPair bra = a.bra[q.x];
+    const GPair ket = a.ket[q.y];
+    Real e[{len(outs)}];
+    if constexpr (F32) eri_{g.tag}_f32_r{r}(bra, ket, a.prims, sboys, e);
+    else eri_{g.tag}_r{r}(bra, ket, a.prims, sboys, e);
+    double mx = 0.0;
+{stores}
+    a.mx[(size_t){r} * a.stride + t] = mx;
+}}""")
+        reg.append(f"    k->mode = 1;\n    k->nacc = 0;\n    k->nrole_a = 0;\n    k->nrole_b = {len(roles)};")
+        for r in range(len(roles)):
+            reg.append(f"    k->sb64[{r}] = k_s2_{g.tag}_r{r}<false>;\n    k->sb32[{r}] = k_s2_{g.tag}_r{r}<true>;")
+        reg.append(f"    k->scat = k_scatter_staged<{NA}, {NB}, {NC}, {ND}>;")
         if bi == ki:
-            reg += (f"    k->diag0 = k_diag<Cls_{g.tag}, 0>;\n    k->diag1 = k_diag<Cls_{g.tag}, 1>;\n"
-                    f"    k->dg_threads = ND_THREADS;\n    k->dg_ppb = ND_THREADS;\n")
-        kern = ""
+            # the diagonal builders keep the block-cooperative role kernels
+            for r, outs in enumerate(roles):
+                funcs.append(g.emit_scatter(f"scat_{g.tag}_r{r}", outs))
+            kern.append(role_kernels(g, roles, True, diag_only=True))
+            reg.append(f"    k->diag0 = k_dg_{g.tag}<0>;\n    k->diag1 = k_dg_{g.tag}<1>;")
+            reg.append(f"    k->dg_threads = {32 * len(roles)};\n    k->dg_ppb = 32;")
+        info.update(roles=len(roles), role_sizes=[len(x) for x in roles], role_outs=roles, acc_groups=[])
     else:
-        reg = (f"    k->nd64 = k_nd_{g.tag}<false>;\n    k->nd32 = k_nd_{g.tag}<true>;\n"
-               f"    k->nd_threads = {32 * R};\n    k->nd_qpb = 32;\n")
+        mode = "staged3"
+        groups = acc_groups(g)
+        keyidx = {}
+        for gr in groups:
+            for key in gr:
+                keyidx[key] = len(keyidx)
+        base = 0
+        for r, gr in enumerate(groups):
+            code, _ = g.emit_acc_role(f"acc_{g.tag}_r{r}", gr)
+            code32, _ = g32.emit_acc_role(f"acc_{g.tag}_f32_r{r}", gr)
+            funcs += [code, code32]
+            kern.append(f"""
+template <bool F32>
+__global__ void __launch_bounds__(ND_THREADS, 3) k_sa_{g.tag}_r{r}(StagedArgs a) {{
+    using Real = typename std::conditional<F32, float, double>::type;
+    __shared__ Real sboys[BOYS_NPT * BOYS_K];
+    if constexpr (F32) stage_boys<{g.L}>(sboys, a.boysf);
+    else stage_boys<{g.L}>(sboys, a.boys);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.n) return;
+    const uint2 q = staged_quartet(a, t);
+    const GPair bra = a.bra[q.x];
+    const GPair ket = a.ket[q.y];
+    if constexpr (F32) acc_{g.tag}_f32_r{r}(bra, ket, a.prims, sboys, a.acc + (size_t){base} * a.stride + t, a.stride);
+    else acc_{g.tag}_r{r}(bra, ket, a.prims, sboys, a.acc + (size_t){base} * a.stride + t, a.stride);
+}}""")
+            base += len(gr)
+        outroles = [list(range(i, min(i + OUT_GROUP3, g.nout))) for i in range(0, g.nout, OUT_GROUP3)]
+        for r, outs in enumerate(outroles):
+            code, _ = g.emit_hrr_role(f"hrr_{g.tag}_r{r}", outs, keyidx)
+            funcs.append(code)
+            kern.append(f"""
+__global__ void __launch_bounds__(ND_THREADS) k_sb_{g.tag}_r{r}(StagedArgs a) {{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.n) return;
+    const uint2 q = staged_quartet(a, t);
+    const GPair bra = a.bra[q.x];
+    const GPair ket = a.ket[q.y];
+    a.mx[(size_t){r} * a.stride + t] =
+        hrr_{g.tag}_r{r}(bra, ket, a.acc + t, a.out + (size_t){outs[0]} * a.stride + t, a.stride);
+}}""")
+        reg.append(f"    k->mode = 2;\n    k->nacc = {len(keyidx)};\n    k->nrole_a = {len(groups)};\n"
+                   f"    k->nrole_b = {len(outroles)};")
+        for r in range(len(groups)):
+            reg.append(f"    k->sa64[{r}] = k_sa_{g.tag}_r{r}<false>;\n    k->sa32[{r}] = k_sa_{g.tag}_r{r}<true>;")
+        for r in range(len(outroles)):
+            reg.append(f"    k->sb64[{r}] = k_sb_{g.tag}_r{r};\n    k->sb32[{r}] = k_sb_{g.tag}_r{r};")
+        reg.append(f"    k->scat = k_scatter_staged<{NA}, {NB}, {NC}, {ND}>;")
         if bi == ki:
-            reg += (f"    k->diag0 = k_dg_{g.tag}<0>;\n    k->diag1 = k_dg_{g.tag}<1>;\n"
-                    f"    k->dg_threads = {32 * R};\n    k->dg_ppb = 32;\n")
-        kern = role_kernels(g, roles, bi == ki)
+            # diagonal builders: one thread per pair over the whole block
+            code, _ = g.emit_role(g.name, list(range(g.nout)))
+            funcs.append(code)
+            funcs.append(f"__device__ __forceinline__ void {g32.name}(const GPair&, const GPair&, const GPrim*, "
+                         f"const float*, float*) {{}}")
+            reg.append(f"    k->diag0 = k_diag<Cls_{g.tag}, 0>;\n    k->diag1 = k_diag<Cls_{g.tag}, 1>;")
+            reg.append(f"    k->dg_threads = ND_THREADS;\n    k->dg_ppb = ND_THREADS;")
+        info.update(roles=len(outroles), role_sizes=[len(x) for x in outroles], role_outs=outroles,
+                    acc_groups=[[[list(k[2]), list(k[3]), k[0], k[1]] for k in gr] for gr in groups])
+        assert len(groups) <= MAXR and len(outroles) <= MAXR
+    if mode == "staged2":
+        assert len(roles) <= MAXR
+    info["mode"] = mode
+    info["dims"] = [NA, NB, NC, ND]
     if bi != ki:
-        reg += "    k->diag0 = nullptr;\n    k->diag1 = nullptr;\n"
-    traits = (f"HF_CLASS_TRAITS({ci}, {bi}, {ki}, {g.tag}, {g.nout}, {g.L})\n" if R == 1 else "")
-    cu = CLASS_TU.format(A=g.A, B=g.B, C=g.C, D=g.D, kernels=kern, ci=ci, bi=bi, ki=ki, tag=g.tag,
-                         hdr=f"cls_{ci:02d}_{g.tag}.cuh", nout=g.nout, L=g.L, reg=reg, roles=R, traits=traits)
+        reg.append("    k->diag0 = nullptr;\n    k->diag1 = nullptr;")
+    traits = (f"HF_CLASS_TRAITS({ci}, {bi}, {ki}, {g.tag}, {g.nout}, {g.L})\n"
+              if mode == "direct" or (mode == "staged3" and bi == ki) else "")
+    cuh = CLASS_CUH.format(A=g.A, B=g.B, C=g.C, D=g.D, roles=mode, body="\n\n".join(funcs))
+    cu = CLASS_TU.format(A=g.A, B=g.B, C=g.C, D=g.D, kernels="\n".join(kern), ci=ci, bi=bi, ki=ki, tag=g.tag,
+                         hdr=f"cls_{ci:02d}_{g.tag}.cuh", nout=g.nout, L=g.L, reg="\n".join(reg) + "\n",
+                         roles=mode, traits=traits)
     return cuh, cu, info
 
 
-def role_kernels(g: ClassGen, roles, diag: bool) -> str:
-    """Kernels of a class split into R roles: a block is R warps over 32
-    quartets; warp r evaluates role r of the quartet of its lane.  The
-    post-screen max|e| is reduced across the warps through shared memory."""
+def role_kernels(g: "ClassGen", roles, diag: bool, diag_only: bool = False) -> str:
+    """Diagonal-builder kernels of a class split into R roles: a block is R
+    warps over 32 shell pairs; warp r evaluates role r of the pair of its
+    lane, and the Schwarz max is reduced across the warps through shared
+    memory."""
     R = len(roles)
     nmax = max(len(x) for x in roles)
     tag, L = g.tag, g.L
-    cases = []
+    dcases = []
     for r, outs in enumerate(roles):
-        cases.append(f"        case {r}: if constexpr (F32) eri_{tag}_f32_r{r}(bra, ket, a.prims, sboys, e); "
-                     f"else eri_{tag}_r{r}(bra, ket, a.prims, sboys, e); nloc = {len(outs)}; break;")
-    scat = [f"            case {r}: scat_{tag}_r{r}(e, s, bra, ket, a.P, a.G, a.nb, a.jonly); break;"
-            for r in range(R)]
-    txt = f"""
-template <bool F32>
-__global__ void __launch_bounds__({32 * R}) k_nd_{tag}(NDArgs a) {{
-    using Real = typename std::conditional<F32, float, double>::type;
-    __shared__ Real sboys[BOYS_NPT * BOYS_K];
-    __shared__ double smax[{32 * R}];
-    if constexpr (F32) stage_boys<{L}>(sboys, a.boysf);
-    else stage_boys<{L}>(sboys, a.boys);
-    const int lane = threadIdx.x & 31, role = threadIdx.x >> 5;
-    const int t = blockIdx.x * 32 + lane;
-    const bool valid = t < a.n;
-    const int tt = valid ? t : 0;
-    const uint2 q = a.from_back ? a.quartets[a.cap - 1 - tt] : a.quartets[tt];
-    const GPair bra = a.bra[q.x];
-    const GPair ket = a.ket[q.y];
-    Real e[{nmax}];
-    int nloc = 0;
-    double mx = 0.0;
-    if (valid) {{
-        switch (role) {{
-{chr(10).join(cases)}
-        }}
-#pragma unroll
-        for (int i = 0; i < {nmax}; ++i)
-            if (i < nloc) mx = fmax(mx, (double)fabs(e[i]));
-    }}
-    smax[threadIdx.x] = mx;
-    __syncthreads();
-    double g = 0.0;
-#pragma unroll
-    for (int r = 0; r < {R}; ++r) g = fmax(g, smax[r * 32 + lane]);
-    const bool keep = valid && !(g < a.thr);  // fock_build_non_diag.f90:69
-    if (keep) {{
-        const double s = (bra.sa == bra.sb ? 0.5 : 1.0) * (ket.sa == ket.sb ? 0.5 : 1.0);
-        switch (role) {{
-{chr(10).join(scat)}
-        }}
-    }}
-    if (a.stats && role == 0)
-        warp_add_stats(a.stats, keep ? 1ull : 0ull, valid ? (unsigned long long)(bra.np * ket.np) : 0ull,
-                       (F32 && keep) ? 1ull : 0ull);
-}}
-"""
-    if diag:
-        dcases = []
-        for r, outs in enumerate(roles):
-            dcases.append(f"        case {r}: eri_{tag}_r{r}(pr, pr, a.prims, sboys, e); nloc = {len(outs)}; break;")
-        txt += f"""
+        dcases.append(f"        case {r}: eri_{tag}_r{r}(pr, pr, a.prims, sboys, e); nloc = {len(outs)}; break;")
+    return f"""
 template <int MODE>
 __global__ void __launch_bounds__({32 * R}) k_dg_{tag}(DiagArgs a) {{
     __shared__ double sboys[BOYS_NPT * BOYS_K];
@@ -654,7 +791,6 @@ __global__ void __launch_bounds__({32 * R}) k_dg_{tag}(DiagArgs a) {{
     }}
 }}
 """
-    return txt
 
 
 CLASS_CUH = """// GENERATED by gen_eri.py -- do not edit.
@@ -703,13 +839,14 @@ def main(outdir: str):
     lines = ["// GENERATED by gen_eri.py -- host dispatch of the class functions (tests only).", ""]
     for ci, info in flops.items():
         tag = info["tag"]
+        nout = info["nout"]
         lines.append(f"inline void host_eri_{ci}(const GPair& b, const GPair& k, const GPrim* p, const double* t,")
         lines.append(f"                          const float* tf, double* out, int f32) {{")
-        if info["roles"] == 1:
-            lines.append(f"    if (f32) {{ float o[{info['nout']}]; eri_{tag}_f32(b, k, p, tf, o);")
-            lines.append(f"        for (int i = 0; i < {info['nout']}; ++i) out[i] = o[i]; }}")
+        if info["mode"] == "direct":
+            lines.append(f"    if (f32) {{ float o[{nout}]; eri_{tag}_f32(b, k, p, tf, o);")
+            lines.append(f"        for (int i = 0; i < {nout}; ++i) out[i] = o[i]; }}")
             lines.append(f"    else eri_{tag}(b, k, p, t, out);")
-        else:
+        elif info["mode"] == "staged2":
             for r, outs in enumerate(info["role_outs"]):
                 n = len(outs)
                 idx = ", ".join(map(str, outs))
@@ -717,26 +854,31 @@ def main(outdir: str):
                 lines.append(f"      if (f32) {{ eri_{tag}_f32_r{r}(b, k, p, tf, of); for (int i = 0; i < {n}; ++i) o[i] = of[i]; }}")
                 lines.append(f"      else eri_{tag}_r{r}(b, k, p, t, o);")
                 lines.append(f"      for (int i = 0; i < {n}; ++i) out[ix[i]] = o[i]; }}")
+        else:
+            nacc = sum(len(g) for g in info["acc_groups"])
+            lines.append(f"    static double acc[{nacc}];")
+            base = 0
+            for r, gr in enumerate(info["acc_groups"]):
+                lines.append(f"    if (f32) acc_{tag}_f32_r{r}(b, k, p, tf, acc + {base}, 1);")
+                lines.append(f"    else acc_{tag}_r{r}(b, k, p, t, acc + {base}, 1);")
+                base += len(gr)
+            for r, outs in enumerate(info["role_outs"]):
+                lines.append(f"    hrr_{tag}_r{r}(b, k, acc, out + {outs[0]}, 1);")
         lines.append("}")
+        # the J/K scatter of a full block with stride 1
+        na, nb_, nc, nd = info["dims"]
         lines.append(f"inline int host_scatter_{ci}(const double* e, double s, const GPair& b, const GPair& k,")
         lines.append(f"                             const double* P, double* G, int nb, bool jonly) {{")
-        if info["roles"] == 1:
-            lines.append("    return 1;")
-        else:
-            for r, outs in enumerate(info["role_outs"]):
-                n = len(outs)
-                idx = ", ".join(map(str, outs))
-                lines.append(f"    {{ static const int ix[{n}] = {{{idx}}}; double o[{n}];")
-                lines.append(f"      for (int i = 0; i < {n}; ++i) o[i] = e[ix[i]];")
-                lines.append(f"      scat_{tag}_r{r}(o, s, b, k, P, G, nb, jonly); }}")
-            lines.append("    return 0;")
+        lines.append(f"    scatter_strided<{na}, {nb_}, {nc}, {nd}>(e, 1, s, b, k, P, G, nb, jonly);")
+        lines.append("    return 0;")
         lines.append("}")
     lines.append("typedef void (*HostEri)(const GPair&, const GPair&, const GPrim*, const double*, const float*, double*, int);")
     lines.append("typedef int (*HostScat)(const double*, double, const GPair&, const GPair&, const double*, double*, int, bool);")
     lines.append("static const HostEri HOST_ERI[] = {" + ", ".join(f"host_eri_{ci}" for ci in flops) + "};")
     lines.append("static const HostScat HOST_SCAT[] = {" + ", ".join(f"host_scatter_{ci}" for ci in flops) + "};")
     txt = "\n".join(lines) + "\n"
-    inc = "".join(f'#include "cls_{ci:02d}_{info["tag"]}.cuh"\n' for ci, info in flops.items())
+    inc = '#include "../scatter.cuh"\n'
+    inc += "".join(f'#include "cls_{ci:02d}_{info["tag"]}.cuh"\n' for ci, info in flops.items())
     inc += "namespace hfgpu {\n#include \"host_dispatch.inc\"\n}\n"
     ai = os.path.join(outdir, "all_classes.inc")
     if not os.path.exists(ai) or open(ai).read() != inc:

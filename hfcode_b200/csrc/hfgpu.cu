@@ -30,6 +30,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <numeric>
@@ -225,6 +226,9 @@ struct hfgpu_handle {
     ScreenClass* d_cls = nullptr;
     uint2* d_q = nullptr;
     size_t qcap = 0;
+    double* d_scratch = nullptr;   // staged classes: accumulators, outputs, maxima
+    size_t scratch_doubles = 0;
+    size_t stride[NCLS] = {};      // quartets per chunk of each staged class
     unsigned long long* d_cnt = nullptr;
     ClassStats* d_stats = nullptr;
     // last build statistics
@@ -328,6 +332,17 @@ int launch_diag(hfgpu_handle* h, int mode, const double* P, double thr, double* 
     return HFGPU_OK;
 }
 
+// Scratch budget of the staged classes in doubles (default 3 GiB; the
+// HFGPU_SCRATCH_MB environment variable overrides it).
+size_t scratch_budget_doubles() {
+    size_t mb = 3072;
+    if (const char* e = getenv("HFGPU_SCRATCH_MB")) {
+        long v = atol(e);
+        if (v > 0) mb = (size_t)v;
+    }
+    return mb * 1024 * 1024 / sizeof(double);
+}
+
 // Schwarz ordering (index_sort + find_threshold) and the active pair arrays.
 int build_active(hfgpu_handle* h) {
     for (int t = 0; t < NPT; ++t) {
@@ -413,7 +428,74 @@ int build_active(hfgpu_handle* h) {
         if (rc) return rc;
         h->qcap = (size_t)std::max<long long>(total_q, 1);
     }
+    // scratch of the staged classes: one chunk of stride quartets holds
+    // (accumulators + outputs + role maxima) doubles per quartet
+    size_t need = 0;
+    const size_t budget = scratch_budget_doubles();
+    for (int c = 0; c < NCLS; ++c) {
+        const ClassKernels& K = CLASS_KERNELS[c];
+        h->stride[c] = 0;
+        if (K.mode == 0 || h->hcls[c].cap == 0) continue;
+        const size_t per = (size_t)K.nacc + K.nout + K.nrole_b;
+        size_t st = std::min<size_t>((size_t)h->hcls[c].cap, budget / per);
+        st = std::max<size_t>(st, 128);
+        h->stride[c] = st;
+        need = std::max(need, st * per);
+    }
+    if (need > h->scratch_doubles) {
+        if (h->d_scratch) cudaFree(h->d_scratch);
+        h->d_scratch = nullptr;
+        h->scratch_doubles = 0;
+        int rc = dalloc(&h->d_scratch, need);
+        if (rc) return rc;
+        h->scratch_doubles = need;
+    }
     h->have_schwarz = true;
+    return HFGPU_OK;
+}
+
+// Staged class: chunks of the quartet list through the accumulator roles
+// (mode 2), the output roles and the scatter kernel.
+int run_staged(hfgpu_handle* h, int c, int prec, long long n, const double* P, double thr, int jonly) {
+    const ClassKernels& K = CLASS_KERNELS[c];
+    const size_t st = h->stride[c];
+    for (long long q0 = 0; q0 < n; q0 += (long long)st) {
+        const int m = (int)std::min<long long>((long long)st, n - q0);
+        StagedArgs a;
+        a.quartets = h->d_q + h->hcls[c].qoff;
+        a.n = m;
+        a.q0 = q0;
+        a.from_back = prec;
+        a.cap = h->hcls[c].cap;
+        a.bra = h->d_apairs[K.bi];
+        a.ket = h->d_apairs[K.ki];
+        a.prims = h->d_prims;
+        a.boys = h->d_boys;
+        a.boysf = h->d_boysf;
+        a.acc = h->d_scratch;
+        a.out = h->d_scratch + (size_t)K.nacc * st;
+        a.mx = h->d_scratch + (size_t)(K.nacc + K.nout) * st;
+        a.stride = st;
+        a.nroles = K.nrole_b;
+        a.P = P;
+        a.G = h->d_G;
+        a.nb = h->nb;
+        a.thr = thr;
+        a.jonly = jonly;
+        a.f32 = prec;
+        a.stats = h->d_stats + c;
+        const int blocks = (m + ND_THREADS - 1) / ND_THREADS;
+        for (int r = 0; r < K.nrole_a; ++r) {
+            (prec ? K.sa32[r] : K.sa64[r])<<<blocks, ND_THREADS, 0, h->stream>>>(a);
+            HF_CHECK(cudaGetLastError());
+        }
+        for (int r = 0; r < K.nrole_b; ++r) {
+            (prec ? K.sb32[r] : K.sb64[r])<<<blocks, ND_THREADS, 0, h->stream>>>(a);
+            HF_CHECK(cudaGetLastError());
+        }
+        K.scat<<<blocks, ND_THREADS, 0, h->stream>>>(a);
+        HF_CHECK(cudaGetLastError());
+    }
     return HFGPU_OK;
 }
 
@@ -441,12 +523,18 @@ int run_non_diag(hfgpu_handle* h, const double* P, double thr, int jonly, double
         for (int prec = 0; prec < 2; ++prec) {
             long long n = (long long)cnt[2 * c + prec];
             if (n == 0) continue;
-            NDArgs a{h->d_q + h->hcls[c].qoff, (int)n, prec, h->hcls[c].cap, h->d_apairs[K.bi], h->d_apairs[K.ki],
-                     h->d_prims, h->d_boys, h->d_boysf, P, h->d_G, h->nb, thr, jonly, h->d_stats + c};
-            long long blocks = (n + K.nd_qpb - 1) / K.nd_qpb;
             if (h->timing) HF_CHECK(cudaEventRecord(h->ev[2 * c], h->stream));
-            (prec ? K.nd32 : K.nd64)<<<(int)blocks, K.nd_threads, 0, h->stream>>>(a);
-            HF_CHECK(cudaGetLastError());
+            if (K.mode == 0) {
+                NDArgs a{h->d_q + h->hcls[c].qoff, (int)n, prec, h->hcls[c].cap, h->d_apairs[K.bi],
+                         h->d_apairs[K.ki], h->d_prims, h->d_boys, h->d_boysf, P, h->d_G, h->nb, thr, jonly,
+                         h->d_stats + c};
+                long long blocks = (n + K.nd_qpb - 1) / K.nd_qpb;
+                (prec ? K.nd32 : K.nd64)<<<(int)blocks, K.nd_threads, 0, h->stream>>>(a);
+                HF_CHECK(cudaGetLastError());
+            } else {
+                int rc = run_staged(h, c, prec, n, P, thr, jonly);
+                if (rc) return rc;
+            }
             if (h->timing) {
                 HF_CHECK(cudaEventRecord(h->ev[2 * c + 1], h->stream));
                 HF_CHECK(cudaEventSynchronize(h->ev[2 * c + 1]));
@@ -568,7 +656,7 @@ int hfgpu_finalize(hfgpu_handle* h) {
     if (!h) return HFGPU_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
     void* bufs[] = {h->d_shtyp, h->d_aosh, h->d_prims, h->d_boys, h->d_boysf, h->d_P, h->d_F, h->d_G,
-                    h->d_md, h->d_cls, h->d_q, h->d_cnt, h->d_stats};
+                    h->d_md, h->d_cls, h->d_q, h->d_cnt, h->d_stats, h->d_scratch};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (int t = 0; t < NPT; ++t) {

@@ -34,7 +34,7 @@ def _build():
     sys.path.pop(0)
     gen_eri.main(GEN)
     srcs = [os.path.join(ROOT, "tests", "hostcheck", "host_eri.cpp"), os.path.join(CSRC, "types.cuh"),
-            os.path.join(CSRC, "pairs.hpp")] + sorted(
+            os.path.join(CSRC, "pairs.hpp"), os.path.join(CSRC, "scatter.cuh")] + sorted(
         os.path.join(GEN, f) for f in os.listdir(GEN) if f.endswith((".cuh", ".inc")))
     h = hashlib.sha1()
     for s in srcs:
@@ -106,7 +106,7 @@ def test_generated_eri_matches_oracle(host):
             assert np.max(np.abs(out32[:ref.size] - ref)) < 2e-5 * scale, (info[str(ci)]["name"], q)
 
 
-def test_generated_role_scatter_matches_uniform_scatter(host):
+def test_generated_scatter_matches_uniform_scatter(host):
     lib, info = host
     _, _, sh, _ = system("alkane2")
     desc = BasisDescriptor(sh)
@@ -118,8 +118,6 @@ def test_generated_role_scatter_matches_uniform_scatter(host):
     P = np.asfortranarray(P + P.T)
     checked = 0
     for ci, qs in class_quartets(sh, rng, n=2).items():
-        if info[str(ci)]["roles"] == 1:
-            continue
         for q in qs:
             e = orc.eri(*q)
             na, nb_, nc, nd = (4 if sh.shtyp[s] == 12 else 5 if sh.shtyp[s] == 3 else 1 for s in q)
