@@ -301,6 +301,10 @@ struct StagedArgs {
     int jonly;
     int f32;
     ClassStats* stats;
+    // diagonal builders only
+    double* schw;          // per pair (MODE 0 writes, MODE 1 reads)
+    const double* md;      // nsh x nsh density maxima
+    int nsh;
 };
 
 __device__ __forceinline__ uint2 staged_quartet(const StagedArgs& a, int t) {
@@ -330,6 +334,37 @@ __global__ void __launch_bounds__(ND_THREADS) k_scatter_staged(StagedArgs a) {
     if (a.stats) warp_add_stats(a.stats, nsc, npr, a.f32 ? nsc : 0ull);
 }
 
+// Diagonal builders of a staged class (quartets (ab|ab), one per pair):
+// MODE 0 writes the Schwarz factor sqrt(max|e|) (fock_build_initial_diag),
+// MODE 1 applies the density screen schw^2 max(D_ab, D_aa/4, D_bb/4) < thr
+// (fock_build_diag.f90:20-21); both skip elements with |e| <= 1e-10 and
+// scatter with the weight (bra perms)^2/8.
+template <int NA, int NB, int MODE>
+__global__ void __launch_bounds__(ND_THREADS) k_scatter_diag(StagedArgs a) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.n) return;
+    const uint2 q = staged_quartet(a, t);
+    const GPair pr = a.bra[q.x];
+    if (MODE == 0) {
+        double m = 0.0;
+        for (int r = 0; r < a.nroles; ++r) m = fmax(m, a.mx[(size_t)r * a.stride + t]);
+        a.schw[q.x] = sqrt(m);
+    } else {
+        const double mv = fmax(a.md[pr.sa * a.nsh + pr.sb],
+                               fmax(0.25 * a.md[pr.sb * a.nsh + pr.sb], 0.25 * a.md[pr.sa * a.nsh + pr.sa]));
+        const double sw = a.schw[q.x];
+        if (sw * sw * mv < a.thr) return;
+    }
+    double* e = a.out + t;
+#pragma unroll 1
+    for (int i = 0; i < NA * NB * NA * NB; ++i) {
+        const double v = e[(size_t)i * a.stride];
+        if (!(fabs(v) > INTTHRESH)) e[(size_t)i * a.stride] = 0.0;  // element skip
+    }
+    const double f = pr.sa == pr.sb ? 1.0 : 2.0;
+    scatter_strided<NA, NB, NA, NB>(e, a.stride, f * f / 8.0, pr, pr, a.P, a.G, a.nb, false);
+}
+
 typedef void (*NDKernel)(NDArgs);
 typedef void (*DiagKernel)(DiagArgs);
 typedef void (*StagedKernel)(StagedArgs);
@@ -347,6 +382,7 @@ struct ClassKernels {
     int dg_threads, dg_ppb;   // block size and pairs per block (diag)
     int nacc, nrole_a, nrole_b;
     StagedKernel sa64[MAXR], sa32[MAXR], sb64[MAXR], sb32[MAXR], scat;
+    StagedKernel dscat0, dscat1;  // staged diagonal builders (classes (X|X))
     int bi, ki, L, nout;
 };
 

@@ -651,12 +651,8 @@ __global__ void __launch_bounds__(ND_THREADS, 3) k_s2_{g.tag}_r{r}(StagedArgs a)
             reg.append(f"    k->sb64[{r}] = k_s2_{g.tag}_r{r}<false>;\n    k->sb32[{r}] = k_s2_{g.tag}_r{r}<true>;")
         reg.append(f"    k->scat = k_scatter_staged<{NA}, {NB}, {NC}, {ND}>;")
         if bi == ki:
-            # the diagonal builders keep the block-cooperative role kernels
-            for r, outs in enumerate(roles):
-                funcs.append(g.emit_scatter(f"scat_{g.tag}_r{r}", outs))
-            kern.append(role_kernels(g, roles, True, diag_only=True))
-            reg.append(f"    k->diag0 = k_dg_{g.tag}<0>;\n    k->diag1 = k_dg_{g.tag}<1>;")
-            reg.append(f"    k->dg_threads = {32 * len(roles)};\n    k->dg_ppb = 32;")
+            reg.append(f"    k->diag0 = nullptr;\n    k->diag1 = nullptr;")
+            reg.append(f"    k->dscat0 = k_scatter_diag<{NA}, {NB}, 0>;\n    k->dscat1 = k_scatter_diag<{NA}, {NB}, 1>;")
         info.update(roles=len(roles), role_sizes=[len(x) for x in roles], role_outs=roles, acc_groups=[])
     else:
         mode = "staged3"
@@ -708,13 +704,8 @@ __global__ void __launch_bounds__(ND_THREADS) k_sb_{g.tag}_r{r}(StagedArgs a) {{
             reg.append(f"    k->sb64[{r}] = k_sb_{g.tag}_r{r};\n    k->sb32[{r}] = k_sb_{g.tag}_r{r};")
         reg.append(f"    k->scat = k_scatter_staged<{NA}, {NB}, {NC}, {ND}>;")
         if bi == ki:
-            # diagonal builders: one thread per pair over the whole block
-            code, _ = g.emit_role(g.name, list(range(g.nout)))
-            funcs.append(code)
-            funcs.append(f"__device__ __forceinline__ void {g32.name}(const GPair&, const GPair&, const GPrim*, "
-                         f"const float*, float*) {{}}")
-            reg.append(f"    k->diag0 = k_diag<Cls_{g.tag}, 0>;\n    k->diag1 = k_diag<Cls_{g.tag}, 1>;")
-            reg.append(f"    k->dg_threads = ND_THREADS;\n    k->dg_ppb = ND_THREADS;")
+            reg.append(f"    k->diag0 = nullptr;\n    k->diag1 = nullptr;")
+            reg.append(f"    k->dscat0 = k_scatter_diag<{NA}, {NB}, 0>;\n    k->dscat1 = k_scatter_diag<{NA}, {NB}, 1>;")
         info.update(roles=len(outroles), role_sizes=[len(x) for x in outroles], role_outs=outroles,
                     acc_groups=[[[list(k[2]), list(k[3]), k[0], k[1]] for k in gr] for gr in groups])
         assert len(groups) <= MAXR and len(outroles) <= MAXR
@@ -724,8 +715,9 @@ __global__ void __launch_bounds__(ND_THREADS) k_sb_{g.tag}_r{r}(StagedArgs a) {{
     info["dims"] = [NA, NB, NC, ND]
     if bi != ki:
         reg.append("    k->diag0 = nullptr;\n    k->diag1 = nullptr;")
-    traits = (f"HF_CLASS_TRAITS({ci}, {bi}, {ki}, {g.tag}, {g.nout}, {g.L})\n"
-              if mode == "direct" or (mode == "staged3" and bi == ki) else "")
+    if not (bi == ki and mode != "direct"):
+        reg.append("    k->dscat0 = nullptr;\n    k->dscat1 = nullptr;")
+    traits = f"HF_CLASS_TRAITS({ci}, {bi}, {ki}, {g.tag}, {g.nout}, {g.L})\n" if mode == "direct" else ""
     cuh = CLASS_CUH.format(A=g.A, B=g.B, C=g.C, D=g.D, roles=mode, body="\n\n".join(funcs))
     cu = CLASS_TU.format(A=g.A, B=g.B, C=g.C, D=g.D, kernels="\n".join(kern), ci=ci, bi=bi, ki=ki, tag=g.tag,
                          hdr=f"cls_{ci:02d}_{g.tag}.cuh", nout=g.nout, L=g.L, reg="\n".join(reg) + "\n",

@@ -227,6 +227,9 @@ struct hfgpu_handle {
     uint2* d_q = nullptr;
     size_t qcap = 0;
     double* d_scratch = nullptr;   // staged classes: accumulators, outputs, maxima
+    uint2* d_diaglist[NPT] = {};   // (i, i) for every pair of a type: staged diagonal builders
+    double* d_dscratch = nullptr;  // scratch of the staged diagonal builders
+    size_t dstride[NPT] = {};
     size_t scratch_doubles = 0;
     size_t stride[NCLS] = {};      // quartets per chunk of each staged class
     unsigned long long* d_cnt = nullptr;
@@ -289,6 +292,8 @@ DiagKernel diag_kernel(int pt, int mode) {
     return mode ? k.diag1 : k.diag0;
 }
 
+size_t scratch_budget_doubles();
+
 int upload_fp(hfgpu_handle* h, const double* f, const double* p) {
     size_t bytes = (size_t)h->nb * h->nb * sizeof(double);
     HF_CHECK(cudaMemcpyAsync(h->d_P, p, bytes, cudaMemcpyHostToDevice, h->stream));
@@ -318,11 +323,63 @@ int launch_symm(hfgpu_handle* h, double* F, const double* G = nullptr) {
     return HFGPU_OK;
 }
 
+// Diagonal builder of a staged pair type: chunks of its pairs through the
+// class's roles and k_scatter_diag.
+int run_staged_diag(hfgpu_handle* h, int t, int mode, const double* P, double thr, double* G, const double* md) {
+    const ClassKernels& K = CLASS_KERNELS[class_index(t, t)];
+    const long long n = (long long)h->pairs[t].size();
+    const size_t st = h->dstride[t];
+    for (long long q0 = 0; q0 < n; q0 += (long long)st) {
+        const int m = (int)std::min<long long>((long long)st, n - q0);
+        StagedArgs a{};
+        a.quartets = h->d_diaglist[t];
+        a.n = m;
+        a.q0 = q0;
+        a.from_back = 0;
+        a.cap = n;
+        a.bra = h->d_pairs[t];
+        a.ket = h->d_pairs[t];
+        a.prims = h->d_prims;
+        a.boys = h->d_boys;
+        a.boysf = h->d_boysf;
+        a.acc = h->d_dscratch;
+        a.out = h->d_dscratch + (size_t)K.nacc * st;
+        a.mx = h->d_dscratch + (size_t)(K.nacc + K.nout) * st;
+        a.stride = st;
+        a.nroles = K.nrole_b;
+        a.P = P;
+        a.G = G;
+        a.nb = h->nb;
+        a.thr = thr;
+        a.stats = nullptr;
+        a.schw = h->d_schw[t];
+        a.md = md;
+        a.nsh = h->nsh;
+        const int blocks = (m + ND_THREADS - 1) / ND_THREADS;
+        for (int r = 0; r < K.nrole_a; ++r) {
+            K.sa64[r]<<<blocks, ND_THREADS, 0, h->stream>>>(a);
+            HF_CHECK(cudaGetLastError());
+        }
+        for (int r = 0; r < K.nrole_b; ++r) {
+            K.sb64[r]<<<blocks, ND_THREADS, 0, h->stream>>>(a);
+            HF_CHECK(cudaGetLastError());
+        }
+        (mode ? K.dscat1 : K.dscat0)<<<blocks, ND_THREADS, 0, h->stream>>>(a);
+        HF_CHECK(cudaGetLastError());
+    }
+    return HFGPU_OK;
+}
+
 int launch_diag(hfgpu_handle* h, int mode, const double* P, double thr, double* G = nullptr,
                 const double* md = nullptr) {
     for (int t = 0; t < NPT; ++t) {
         int n = (int)h->pairs[t].size();
         if (n == 0) continue;
+        if (CLASS_KERNELS[class_index(t, t)].mode != 0) {
+            int rc = run_staged_diag(h, t, mode, P, thr, G ? G : h->d_G, md ? md : h->d_md);
+            if (rc) return rc;
+            continue;
+        }
         DiagArgs a{h->d_pairs[t], n, h->d_prims, h->d_boys, h->d_schw[t], md ? md : h->d_md, h->nsh, P,
                    G ? G : h->d_G, h->nb, thr};
         const ClassKernels& K = CLASS_KERNELS[class_index(t, t)];
@@ -642,7 +699,32 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
         hfgpu_finalize(h);
         return set_err(HFGPU_ERR_CUDA, m);
     }
-    ce = cudaDeviceSynchronize();
+    // staged diagonal builders: (i, i) lists and their scratch
+    {
+        size_t need = 0;
+        const size_t budget = scratch_budget_doubles();
+        for (int t = 0; t < NPT && ce == cudaSuccess; ++t) {
+            const ClassKernels& K = CLASS_KERNELS[class_index(t, t)];
+            const size_t n = h->pairs[t].size();
+            if (K.mode == 0 || n == 0) continue;
+            std::vector<uint2> dl(n);
+            for (size_t i = 0; i < n; ++i) dl[i] = make_uint2((unsigned)i, (unsigned)i);
+            if (dalloc(&h->d_diaglist[t], n)) {
+                hfgpu_finalize(h);
+                return HFGPU_ERR_NOMEM;
+            }
+            ce = up(h->d_diaglist[t], dl.data(), n * sizeof(uint2));
+            const size_t per = (size_t)K.nacc + K.nout + K.nrole_b;
+            size_t st = std::max<size_t>(std::min<size_t>(n, budget / per), 128);
+            h->dstride[t] = st;
+            need = std::max(need, st * per);
+        }
+        if (ce == cudaSuccess && need && dalloc(&h->d_dscratch, need)) {
+            hfgpu_finalize(h);
+            return HFGPU_ERR_NOMEM;
+        }
+    }
+    if (ce == cudaSuccess) ce = cudaDeviceSynchronize();
     if (ce != cudaSuccess) {
         std::string m = std::string("hfgpu_init: ") + cudaGetErrorString(ce);
         hfgpu_finalize(h);
@@ -656,11 +738,11 @@ int hfgpu_finalize(hfgpu_handle* h) {
     if (!h) return HFGPU_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
     void* bufs[] = {h->d_shtyp, h->d_aosh, h->d_prims, h->d_boys, h->d_boysf, h->d_P, h->d_F, h->d_G,
-                    h->d_md, h->d_cls, h->d_q, h->d_cnt, h->d_stats, h->d_scratch};
+                    h->d_md, h->d_cls, h->d_q, h->d_cnt, h->d_stats, h->d_scratch, h->d_dscratch};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (int t = 0; t < NPT; ++t) {
-        void* tb[] = {h->d_pairs[t], h->d_schw[t], h->d_apairs[t], h->d_ash[t], h->d_aschw[t]};
+        void* tb[] = {h->d_pairs[t], h->d_schw[t], h->d_apairs[t], h->d_ash[t], h->d_aschw[t], h->d_diaglist[t]};
         for (void* b : tb)
             if (b) cudaFree(b);
     }
