@@ -66,6 +66,9 @@ thread_local std::string g_err;
     } while (0)
 
 constexpr double SHTHRESH = 1e-11;      // molprops.f90:163
+// bra and ket pair types of the 21 quartet classes (pair types i <= j, row by row)
+__constant__ int CLS_BI[NCLS] = {0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 1, 2, 2, 2, 2, 3, 3, 3, 4, 4, 5};
+__constant__ int CLS_KI[NCLS] = {0, 1, 2, 3, 4, 5, 1, 2, 3, 4, 5, 2, 3, 4, 5, 3, 4, 5, 4, 5, 5};
 
 // evaluate_maxdm.f90: one thread per unordered shell pair.
 __global__ void k_maxdm(const int* __restrict__ shtyp, const int* __restrict__ aosh, int nsh, int nb,
@@ -94,75 +97,99 @@ __global__ void k_maxdm(const int* __restrict__ shtyp, const int* __restrict__ a
     md[(size_t)b * nsh + a] = m;
 }
 
-struct ScreenClass {
-    long long start;   // first padded candidate index of this class
+// One screening sub-class: the candidates of quartet class `cls` whose bra
+// pairs come from one primitive-count group of the active bra list and ket
+// pairs from one group of the ket list, so that every quartet in the
+// compacted sub-list runs its primitive loops with the same trip counts.
+struct ScreenSub {
+    long long start;   // first padded candidate index
     long long ncand;   // candidates (unpadded)
-    long long cap;     // slots in the quartet list segment
-    long long qoff;    // offset of the segment
-    int same;          // bra type == ket type (triangular enumeration)
-    int nket;
-    const int2* bsh;   // (sa, sb) per active bra pair
-    const int2* ksh;
-    const double* bschw;
-    const double* kschw;
+    int cls;
+    int same;          // one group against itself: pairs i > j only
+    int b0, nbra;      // bra range in the active list
+    int k0, nket;      // ket range
+    long long off[2];  // write offsets of the FP64 / FP32 entries (second pass)
 };
 
-// Per-quartet screen of fock_build_non_diag.f90:63-67, compacted into the
-// class's list.  Candidates of each class are padded to a multiple of 32 so a
-// warp never spans two classes.
-__global__ void k_screen(const ScreenClass* __restrict__ cls, int ncls, long long ntot,
-                         const double* __restrict__ md, int nsh, double thr, int jonly, double f32cut,
-                         uint2* __restrict__ qbuf, unsigned long long* __restrict__ cnt) {
-    __shared__ ScreenClass sc[NCLS];
-    for (int i = threadIdx.x; i < ncls; i += blockDim.x) sc[i] = cls[i];
-    __syncthreads();
+struct ScreenArgs {
+    const ScreenSub* subs;
+    int nsub;
+    long long ntot;
+    const int2* sh[NPT];      // (sa, sb) per active pair, per pair type
+    const double* schw[NPT];  // Schwarz factor per active pair
+    const double* md;
+    int nsh;
+    double thr;
+    int jonly;
+    double f32cut;
+    unsigned long long* cnt;  // [2*nsub]: pass 1 counts, pass 2 positions
+    uint2* qbuf;
+};
+
+// Per-quartet screen of fock_build_non_diag.f90:63-67 over every candidate
+// pair of active shell pairs.  PASS 0 counts the survivors of each
+// sub-class (FP64 and FP32 separately); PASS 1 writes them compacted at the
+// offsets the host derived from those counts.  Candidates of each sub-class
+// are padded to a multiple of 32 so a warp never spans two sub-classes.
+template <int PASS>
+__global__ void k_screen(ScreenArgs a) {
     const int lane = threadIdx.x & 31;
     const long long nwarps_total = (long long)gridDim.x * (blockDim.x >> 5);
-    for (long long w = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); w * 32 < ntot;
+    for (long long w = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); w * 32 < a.ntot;
          w += nwarps_total) {
-        const long long t = w * 32 + lane;
         const long long w0 = w * 32;
-        int c = 0;
-        while (c + 1 < ncls && sc[c + 1].start <= w0) ++c;
-        const ScreenClass& C = sc[c];
-        const long long u = t - C.start;
+        int lo_i = 0, hi_i = a.nsub - 1;  // last sub with start <= w0
+        while (lo_i < hi_i) {
+            const int mid = (lo_i + hi_i + 1) >> 1;
+            if (a.subs[mid].start <= w0) lo_i = mid;
+            else hi_i = mid - 1;
+        }
+        const int c = lo_i;
+        const ScreenSub S = a.subs[c];
+        const long long u = w0 + lane - S.start;
         bool pass = false, lo = false;
         unsigned ii = 0, jj = 0;
-        if (u < C.ncand) {
-            if (C.same) {
-                long long i = (long long)((1.0 + sqrt(1.0 + 8.0 * (double)u)) * 0.5);
+        if (u < S.ncand) {
+            long long i, j;
+            if (S.same) {
+                i = (long long)((1.0 + sqrt(1.0 + 8.0 * (double)u)) * 0.5);
                 while (i * (i - 1) / 2 > u) --i;
                 while ((i + 1) * i / 2 <= u) ++i;
-                ii = (unsigned)i;
-                jj = (unsigned)(u - i * (i - 1) / 2);
+                j = u - i * (i - 1) / 2;
             } else {
-                ii = (unsigned)(u / C.nket);
-                jj = (unsigned)(u - (long long)ii * C.nket);
+                i = u / S.nket;
+                j = u - i * S.nket;
             }
-            const int2 ab = C.bsh[ii], cd = C.ksh[jj];
-            const double dc = fmax(md[ab.x * nsh + ab.y], md[cd.x * nsh + cd.y]);
+            ii = (unsigned)(S.b0 + i);
+            jj = (unsigned)(S.k0 + j);
+            const int bt = 0;  // pair types are resolved through the class
+            (void)bt;
+            const int2 ab = a.sh[CLS_BI[S.cls]][ii], cd = a.sh[CLS_KI[S.cls]][jj];
+            const double dc = fmax(a.md[ab.x * a.nsh + ab.y], a.md[cd.x * a.nsh + cd.y]);
             double v = dc;
-            if (!jonly) {
-                const double dx = fmax(fmax(md[ab.x * nsh + cd.x], md[ab.x * nsh + cd.y]),
-                                       fmax(md[ab.y * nsh + cd.x], md[ab.y * nsh + cd.y]));
+            if (!a.jonly) {
+                const double dx = fmax(fmax(a.md[ab.x * a.nsh + cd.x], a.md[ab.x * a.nsh + cd.y]),
+                                       fmax(a.md[ab.y * a.nsh + cd.x], a.md[ab.y * a.nsh + cd.y]));
                 v = fmax(dc, 0.25 * dx);
             }
-            const double bound = C.bschw[ii] * C.kschw[jj] * v;
-            pass = !(bound < thr);
-            lo = pass && bound < f32cut;
+            const double bound = a.schw[CLS_BI[S.cls]][ii] * a.schw[CLS_KI[S.cls]][jj] * v;
+            pass = !(bound < a.thr);
+            lo = pass && bound < a.f32cut;
         }
         const unsigned m64 = __ballot_sync(0xffffffffu, pass && !lo);
         const unsigned m32 = __ballot_sync(0xffffffffu, lo);
         unsigned long long b64 = 0, b32 = 0;
         if (lane == 0) {
-            if (m64) b64 = atomicAdd(&cnt[2 * c], (unsigned long long)__popc(m64));
-            if (m32) b32 = atomicAdd(&cnt[2 * c + 1], (unsigned long long)__popc(m32));
+            if (m64) b64 = atomicAdd(&a.cnt[2 * c], (unsigned long long)__popc(m64));
+            if (m32) b32 = atomicAdd(&a.cnt[2 * c + 1], (unsigned long long)__popc(m32));
         }
-        b64 = __shfl_sync(0xffffffffu, b64, 0);
-        b32 = __shfl_sync(0xffffffffu, b32, 0);
-        const unsigned lt = (1u << lane) - 1u;
-        if (pass && !lo) qbuf[C.qoff + (long long)b64 + __popc(m64 & lt)] = make_uint2(ii, jj);
-        if (lo) qbuf[C.qoff + C.cap - 1 - ((long long)b32 + __popc(m32 & lt))] = make_uint2(ii, jj);
+        if (PASS == 1) {
+            b64 = __shfl_sync(0xffffffffu, b64, 0);
+            b32 = __shfl_sync(0xffffffffu, b32, 0);
+            const unsigned lt = (1u << lane) - 1u;
+            if (pass && !lo) a.qbuf[S.off[0] + (long long)b64 + __popc(m64 & lt)] = make_uint2(ii, jj);
+            if (lo) a.qbuf[S.off[1] + (long long)b32 + __popc(m32 & lt)] = make_uint2(ii, jj);
+        }
     }
 }
 
@@ -217,13 +244,16 @@ struct hfgpu_handle {
     int2* d_ash[NPT] = {};
     double* d_aschw[NPT] = {};
     int nact[NPT] = {};
+    std::vector<int> act_np[NPT];
     double* d_boys = nullptr;
     float* d_boysf = nullptr;
     double* d_P = nullptr;
     double* d_F = nullptr;
     double* d_G = nullptr;
     double* d_md = nullptr;
-    ScreenClass* d_cls = nullptr;
+    ScreenSub* d_subs = nullptr;
+    std::vector<ScreenSub> hsubs;
+    size_t subcap = 0;
     uint2* d_q = nullptr;
     size_t qcap = 0;
     double* d_scratch = nullptr;   // staged classes: accumulators, outputs, maxima
@@ -237,8 +267,10 @@ struct hfgpu_handle {
     // last build statistics
     long long st_pass[NCLS] = {}, st_scat[NCLS] = {}, st_prim[NCLS] = {}, st_f32[NCLS] = {};
     double st_ms[NCLS] = {};
-    ScreenClass hcls[NCLS];
     long long ntot = 0;
+    long long ccap[NCLS] = {};      // candidates per class (upper bound of its list)
+    long long coff[NCLS] = {};      // class region in the quartet buffer
+    long long n64[NCLS] = {}, n32[NCLS] = {};
     cudaEvent_t ev[2 * NCLS + 2] = {};
 };
 
@@ -445,6 +477,8 @@ int build_active(hfgpu_handle* h) {
             asc[i] = h->schw[t][act[i]];
         }
         h->nact[t] = last;
+        h->act_np[t].resize(last);
+        for (int i = 0; i < last; ++i) h->act_np[t][i] = ap[i].np;
         if (last) {
             HF_CHECK(cudaMemcpyAsync(h->d_apairs[t], ap.data(), last * sizeof(GPair), cudaMemcpyHostToDevice,
                                      h->stream));
@@ -454,29 +488,57 @@ int build_active(hfgpu_handle* h) {
             HF_CHECK(cudaStreamSynchronize(h->stream));
         }
     }
-    // screening descriptors and quartet-list segments
+    // screening sub-classes: primitive-count groups of the active lists
+    std::vector<std::pair<int, int>> groups[NPT];  // (start, length)
+    for (int t = 0; t < NPT; ++t) {
+        const int n = h->nact[t];
+        for (int i = 0; i < n;) {
+            int j = i + 1;
+            while (j < n && h->act_np[t][j] == h->act_np[t][i]) ++j;
+            groups[t].push_back({i, j - i});
+            i = j;
+        }
+    }
+    h->hsubs.clear();
     long long start = 0, qoff = 0;
     for (int c = 0; c < NCLS; ++c) {
         const int bi = CLASS_KERNELS[c].bi, ki = CLASS_KERNELS[c].ki;
-        ScreenClass& s = h->hcls[c];
-        const long long nb_ = h->nact[bi], nk = h->nact[ki];
-        s.same = bi == ki;
-        s.ncand = s.same ? nb_ * (nb_ - 1) / 2 : nb_ * nk;
-        s.nket = (int)nk;
-        s.start = start;
-        s.cap = s.ncand;
-        s.qoff = qoff;
-        s.bsh = h->d_ash[bi];
-        s.ksh = h->d_ash[ki];
-        s.bschw = h->d_aschw[bi];
-        s.kschw = h->d_aschw[ki];
-        start += (s.ncand + 31) / 32 * 32;
-        qoff += s.cap;
+        long long ccap = 0;
+        for (size_t gb = 0; gb < groups[bi].size(); ++gb)
+            for (size_t gk = 0; gk < groups[ki].size(); ++gk) {
+                if (bi == ki && gk > gb) continue;  // pairs (ii, jj) with ii > jj only
+                ScreenSub sub{};
+                sub.cls = c;
+                sub.same = (bi == ki && gb == gk);
+                sub.b0 = groups[bi][gb].first;
+                sub.nbra = groups[bi][gb].second;
+                sub.k0 = groups[ki][gk].first;
+                sub.nket = groups[ki][gk].second;
+                sub.ncand = sub.same ? (long long)sub.nbra * (sub.nbra - 1) / 2 : (long long)sub.nbra * sub.nket;
+                if (sub.ncand == 0) continue;
+                sub.start = start;
+                start += (sub.ncand + 31) / 32 * 32;
+                ccap += sub.ncand;
+                h->hsubs.push_back(sub);
+            }
+        h->ccap[c] = ccap;
+        h->coff[c] = qoff;
+        qoff += ccap;
     }
     h->ntot = start;
     total_q = qoff;
-    HF_CHECK(cudaMemcpyAsync(h->d_cls, h->hcls, sizeof(h->hcls), cudaMemcpyHostToDevice, h->stream));
-    HF_CHECK(cudaStreamSynchronize(h->stream));
+    if (h->hsubs.size() > h->subcap) {
+        if (h->d_subs) cudaFree(h->d_subs);
+        h->d_subs = nullptr;
+        h->subcap = 0;
+        int rc = dalloc(&h->d_subs, h->hsubs.size());
+        if (rc) return rc;
+        if (h->d_cnt) cudaFree(h->d_cnt);
+        h->d_cnt = nullptr;
+        rc = dalloc(&h->d_cnt, 2 * h->hsubs.size());
+        if (rc) return rc;
+        h->subcap = h->hsubs.size();
+    }
     if ((size_t)total_q > h->qcap) {
         if (h->d_q) cudaFree(h->d_q);
         h->d_q = nullptr;
@@ -492,9 +554,9 @@ int build_active(hfgpu_handle* h) {
     for (int c = 0; c < NCLS; ++c) {
         const ClassKernels& K = CLASS_KERNELS[c];
         h->stride[c] = 0;
-        if (K.mode == 0 || h->hcls[c].cap == 0) continue;
+        if (K.mode == 0 || h->ccap[c] == 0) continue;
         const size_t per = (size_t)K.nacc + K.nout + K.nrole_b;
-        size_t st = std::min<size_t>((size_t)h->hcls[c].cap, budget / per);
+        size_t st = std::min<size_t>((size_t)h->ccap[c], budget / per);
         st = std::max<size_t>(st, 128);
         h->stride[c] = st;
         need = std::max(need, st * per);
@@ -519,11 +581,11 @@ int run_staged(hfgpu_handle* h, int c, int prec, long long n, const double* P, d
     for (long long q0 = 0; q0 < n; q0 += (long long)st) {
         const int m = (int)std::min<long long>((long long)st, n - q0);
         StagedArgs a;
-        a.quartets = h->d_q + h->hcls[c].qoff;
+        a.quartets = h->d_q + h->coff[c] + (prec ? h->n64[c] : 0);
         a.n = m;
         a.q0 = q0;
-        a.from_back = prec;
-        a.cap = h->hcls[c].cap;
+        a.from_back = 0;
+        a.cap = n;
         a.bra = h->d_apairs[K.bi];
         a.ket = h->d_apairs[K.ki];
         a.prims = h->d_prims;
@@ -558,21 +620,71 @@ int run_staged(hfgpu_handle* h, int c, int prec, long long n, const double* P, d
 
 int run_non_diag(hfgpu_handle* h, const double* P, double thr, int jonly, double f32cut) {
     if (!h->have_schwarz) return set_err(HFGPU_ERR_STATE, "fock_build_initial_diag has not been called");
-    HF_CHECK(cudaMemsetAsync(h->d_cnt, 0, 2 * NCLS * sizeof(unsigned long long), h->stream));
     HF_CHECK(cudaMemsetAsync(h->d_stats, 0, NCLS * sizeof(ClassStats), h->stream));
-    if (h->ntot > 0) {
+    const int nsub = (int)h->hsubs.size();
+    for (int c = 0; c < NCLS; ++c) h->n64[c] = h->n32[c] = 0;
+    if (h->ntot > 0 && nsub > 0) {
         int dev = 0, nsm = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        long long warps = h->ntot / 32;
-        long long blocks = std::min<long long>((warps + 7) / 8, (long long)nsm * 64);
-        k_screen<<<(int)blocks, 256, 0, h->stream>>>(h->d_cls, NCLS, h->ntot, h->d_md, h->nsh, thr, jonly, f32cut,
-                                                      h->d_q, h->d_cnt);
+        ScreenArgs sa{};
+        sa.subs = h->d_subs;
+        sa.nsub = nsub;
+        sa.ntot = h->ntot;
+        for (int t = 0; t < NPT; ++t) {
+            sa.sh[t] = h->d_ash[t];
+            sa.schw[t] = h->d_aschw[t];
+        }
+        sa.md = h->d_md;
+        sa.nsh = h->nsh;
+        sa.thr = thr;
+        sa.jonly = jonly;
+        sa.f32cut = f32cut;
+        sa.cnt = h->d_cnt;
+        sa.qbuf = h->d_q;
+        const long long warps = h->ntot / 32;
+        const int blocks = (int)std::min<long long>((warps + 7) / 8, (long long)nsm * 64);
+        // pass 0: survivors per sub-class
+        HF_CHECK(cudaMemsetAsync(h->d_cnt, 0, 2 * nsub * sizeof(unsigned long long), h->stream));
+        HF_CHECK(cudaMemcpyAsync(h->d_subs, h->hsubs.data(), nsub * sizeof(ScreenSub), cudaMemcpyHostToDevice,
+                                 h->stream));
+        k_screen<0><<<blocks, 256, 0, h->stream>>>(sa);
         HF_CHECK(cudaGetLastError());
+        std::vector<unsigned long long> cnt(2 * nsub);
+        HF_CHECK(cudaMemcpyAsync(cnt.data(), h->d_cnt, cnt.size() * sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToHost, h->stream));
+        HF_CHECK(cudaStreamSynchronize(h->stream));
+        // offsets: per class, FP64 entries then FP32 entries, sub-classes in order
+        for (int k = 0; k < nsub; ++k) {
+            const int c = h->hsubs[k].cls;
+            h->n64[c] += (long long)cnt[2 * k];
+            h->n32[c] += (long long)cnt[2 * k + 1];
+        }
+        long long p64[NCLS], p32[NCLS];
+        for (int c = 0; c < NCLS; ++c) {
+            p64[c] = h->coff[c];
+            p32[c] = h->coff[c] + h->n64[c];
+        }
+        for (int k = 0; k < nsub; ++k) {
+            const int c = h->hsubs[k].cls;
+            h->hsubs[k].off[0] = p64[c];
+            h->hsubs[k].off[1] = p32[c];
+            p64[c] += (long long)cnt[2 * k];
+            p32[c] += (long long)cnt[2 * k + 1];
+        }
+        // pass 1: compacted write
+        HF_CHECK(cudaMemsetAsync(h->d_cnt, 0, 2 * nsub * sizeof(unsigned long long), h->stream));
+        HF_CHECK(cudaMemcpyAsync(h->d_subs, h->hsubs.data(), nsub * sizeof(ScreenSub), cudaMemcpyHostToDevice,
+                                 h->stream));
+        k_screen<1><<<blocks, 256, 0, h->stream>>>(sa);
+        HF_CHECK(cudaGetLastError());
+        HF_CHECK(cudaStreamSynchronize(h->stream));  // hsubs is re-used as the copy source
     }
     unsigned long long cnt[2 * NCLS];
-    HF_CHECK(cudaMemcpyAsync(cnt, h->d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, h->stream));
-    HF_CHECK(cudaStreamSynchronize(h->stream));
+    for (int c = 0; c < NCLS; ++c) {
+        cnt[2 * c] = (unsigned long long)h->n64[c];
+        cnt[2 * c + 1] = (unsigned long long)h->n32[c];
+    }
     for (int c = 0; c < NCLS; ++c) {
         const ClassKernels& K = CLASS_KERNELS[c];
         h->st_pass[c] = (long long)(cnt[2 * c] + cnt[2 * c + 1]);
@@ -582,7 +694,7 @@ int run_non_diag(hfgpu_handle* h, const double* P, double thr, int jonly, double
             if (n == 0) continue;
             if (h->timing) HF_CHECK(cudaEventRecord(h->ev[2 * c], h->stream));
             if (K.mode == 0) {
-                NDArgs a{h->d_q + h->hcls[c].qoff, (int)n, prec, h->hcls[c].cap, h->d_apairs[K.bi],
+                NDArgs a{h->d_q + h->coff[c] + (prec ? h->n64[c] : 0), (int)n, 0, n, h->d_apairs[K.bi],
                          h->d_apairs[K.ki], h->d_prims, h->d_boys, h->d_boysf, P, h->d_G, h->nb, thr, jonly,
                          h->d_stats + c};
                 long long blocks = (n + K.nd_qpb - 1) / K.nd_qpb;
@@ -664,7 +776,6 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
     rc |= dalloc(&h->d_F, nb2);
     rc |= dalloc(&h->d_G, nb2);
     rc |= dalloc(&h->d_md, (size_t)h->nsh * h->nsh);
-    rc |= dalloc(&h->d_cls, NCLS);
     rc |= dalloc(&h->d_cnt, 2 * NCLS);
     rc |= dalloc(&h->d_stats, NCLS);
     for (int t = 0; t < NPT; ++t) {
@@ -738,7 +849,7 @@ int hfgpu_finalize(hfgpu_handle* h) {
     if (!h) return HFGPU_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
     void* bufs[] = {h->d_shtyp, h->d_aosh, h->d_prims, h->d_boys, h->d_boysf, h->d_P, h->d_F, h->d_G,
-                    h->d_md, h->d_cls, h->d_q, h->d_cnt, h->d_stats, h->d_scratch, h->d_dscratch};
+                    h->d_md, h->d_subs, h->d_q, h->d_cnt, h->d_stats, h->d_scratch, h->d_dscratch};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (int t = 0; t < NPT; ++t) {
