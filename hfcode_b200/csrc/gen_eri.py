@@ -629,7 +629,7 @@ def class_source(ci: int, bi: int, ki: int):
                                f"mx = fmax(mx, fabs(v)); }}" for i, n in enumerate(outs))
             kern.append(f"""
 template <bool F32>
-__global__ void __launch_bounds__(ND_THREADS, 3) k_s2_{g.tag}_r{r}(StagedArgs a) {{
+__global__ void __launch_bounds__(ND_THREADS, 2) k_s2_{g.tag}_r{r}(StagedArgs a) {{
     using Real = typename std::conditional<F32, float, double>::type;
     __shared__ Real sboys[BOYS_NPT * BOYS_K];
     if constexpr (F32) stage_boys<{g.L}>(sboys, a.boysf);
@@ -668,7 +668,7 @@ __global__ void __launch_bounds__(ND_THREADS, 3) k_s2_{g.tag}_r{r}(StagedArgs a)
             funcs += [code, code32]
             kern.append(f"""
 template <bool F32>
-__global__ void __launch_bounds__(ND_THREADS, 3) k_sa_{g.tag}_r{r}(StagedArgs a) {{
+__global__ void __launch_bounds__(ND_THREADS, 2) k_sa_{g.tag}_r{r}(StagedArgs a) {{
     using Real = typename std::conditional<F32, float, double>::type;
     __shared__ Real sboys[BOYS_NPT * BOYS_K];
     if constexpr (F32) stage_boys<{g.L}>(sboys, a.boysf);
