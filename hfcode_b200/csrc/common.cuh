@@ -19,11 +19,11 @@ __host__ __device__ constexpr int pt_nb(int t) { return t == 0 ? 1 : t == 1 ? 1 
 #define HF_CLASS_TRAITS(ci, bi, ki, NAME, nout, L)                                                   \
     struct Cls_##NAME {                                                                              \
         static constexpr int CI = ci, BI = bi, KI = ki, NOUT = nout, LL = L;                         \
-        __device__ __forceinline__ static void eri(const GPair& b, const GPair& k, const GPrim* p,   \
+        __device__ __forceinline__ static void eri(const GPair& b, const GPair& k, const PrimSoA& p, \
                                                    const double* t, double* o) {                     \
             eri_##NAME(b, k, p, t, o);                                                               \
         }                                                                                            \
-        __device__ __forceinline__ static void eri32(const GPair& b, const GPair& k, const GPrim* p,  \
+        __device__ __forceinline__ static void eri32(const GPair& b, const GPair& k, const PrimSoA& p, \
                                                      const float* t, float* o) {                     \
             eri_##NAME##_f32(b, k, p, t, o);                                                         \
         }                                                                                            \
@@ -160,7 +160,7 @@ struct NDArgs {
     long long cap;
     const GPair* bra;
     const GPair* ket;
-    const GPrim* prims;
+    PrimSoA prims;
     const double* boys;     // global table, [M][225][8]
     const float* boysf;
     const double* P;
@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_nondiag(NDArgs a) {
 struct DiagArgs {
     const GPair* pairs;
     int n;
-    const GPrim* prims;
+    PrimSoA prims;
     const double* boys;
     double* schw;          // mode 0: written; mode 1: read
     const double* md;      // mode 1: nsh x nsh maxdm
@@ -286,7 +286,7 @@ struct StagedArgs {
     long long cap;
     const GPair* bra;
     const GPair* ket;
-    const GPrim* prims;
+    PrimSoA prims;
     const double* boys;
     const float* boysf;
     double* acc;

@@ -311,7 +311,7 @@ class ClassGen:
         w("    const double Ax = bra.A[0], Ay = bra.A[1], Az = bra.A[2];")
         w("    const double Cx = ket.A[0], Cy = ket.A[1], Cz = ket.A[2];")
         w("    for (int ib = 0; ib < bra.np; ++ib) {")
-        w("        const GPrim pb = prims[bra.p0 + ib];")
+        w("        const GPrim pb = load_prim(prims, bra.p0 + ib * bra.ps);")
         w(f"        const {ft} p = {cv('pb.p')};")
         w(f"        const {ft} PA0 = {cv('pb.P[0] - Ax')}, PA1 = {cv('pb.P[1] - Ay')}, PA2 = {cv('pb.P[2] - Az')};")
         used_b = sorted({k[0] for k in acc})
@@ -321,7 +321,7 @@ class ClassGen:
             expr = " * ".join(cv(f"pb.w{x}") for x in wt) if wt else "1"
             w(f"        const {ft} wb{bi} = {expr};")
         w("        for (int ik = 0; ik < ket.np; ++ik) {")
-        w("            const GPrim pk = prims[ket.p0 + ik];")
+        w("            const GPrim pk = load_prim(prims, ket.p0 + ik * ket.ps);")
         w(f"            const {ft} q = {cv('pk.p')};")
         one = "1.0" if dbl else "1.0f"
         half = "0.5" if dbl else "0.5f"
@@ -448,7 +448,7 @@ class ClassGen:
         out = [f"// ({self.A}{self.B}|{self.C}{self.D}) outputs {outs[0]}..{outs[-1]} ({len(outs)}): L={self.L}, "
                f"{vst['acc']} accumulators, VRR {vst['vrr']} terms ({vst['order']}-first)",
                f"__device__ __forceinline__ void {fname}(const GPair& bra, const GPair& ket,",
-               f"    const GPrim* __restrict__ prims, const {ft}* __restrict__ btab, {ft}* __restrict__ out)",
+               f"    const PrimSoA& prims, const {ft}* __restrict__ btab, {ft}* __restrict__ out)",
                "{"]
         out += vlines + hlines
         out += [f"    out[{r}] = {v};" for r, v in enumerate(vals)]
@@ -463,7 +463,7 @@ class ClassGen:
         out = [f"// ({self.A}{self.B}|{self.C}{self.D}) accumulators ({len(keys)}): VRR {vst['vrr']} terms "
                f"({vst['order']}-first)",
                f"__device__ __forceinline__ void {fname}(const GPair& bra, const GPair& ket,",
-               f"    const GPrim* __restrict__ prims, const {ft}* __restrict__ btab, double* __restrict__ dst, "
+               f"    const PrimSoA& prims, const {ft}* __restrict__ btab, double* __restrict__ dst, "
                f"size_t stride)",
                "{"]
         out += vlines
@@ -832,7 +832,7 @@ def main(outdir: str):
     for ci, info in flops.items():
         tag = info["tag"]
         nout = info["nout"]
-        lines.append(f"inline void host_eri_{ci}(const GPair& b, const GPair& k, const GPrim* p, const double* t,")
+        lines.append(f"inline void host_eri_{ci}(const GPair& b, const GPair& k, const PrimSoA& p, const double* t,")
         lines.append(f"                          const float* tf, double* out, int f32) {{")
         if info["mode"] == "direct":
             lines.append(f"    if (f32) {{ float o[{nout}]; eri_{tag}_f32(b, k, p, tf, o);")
@@ -864,7 +864,7 @@ def main(outdir: str):
         lines.append(f"    scatter_strided<{na}, {nb_}, {nc}, {nd}>(e, 1, s, b, k, P, G, nb, jonly);")
         lines.append("    return 0;")
         lines.append("}")
-    lines.append("typedef void (*HostEri)(const GPair&, const GPair&, const GPrim*, const double*, const float*, double*, int);")
+    lines.append("typedef void (*HostEri)(const GPair&, const GPair&, const PrimSoA&, const double*, const float*, double*, int);")
     lines.append("typedef int (*HostScat)(const double*, double, const GPair&, const GPair&, const double*, double*, int, bool);")
     lines.append("static const HostEri HOST_ERI[] = {" + ", ".join(f"host_eri_{ci}" for ci in flops) + "};")
     lines.append("static const HostScat HOST_SCAT[] = {" + ", ".join(f"host_scatter_{ci}" for ci in flops) + "};")

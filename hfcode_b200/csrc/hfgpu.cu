@@ -237,7 +237,11 @@ struct hfgpu_handle {
     // device
     int* d_shtyp = nullptr;
     int* d_aosh = nullptr;
-    GPrim* d_prims = nullptr;
+    double* d_psoa = nullptr;      // all-pairs primitive arrays (SoA)
+    PrimSoA psoa{};
+    double* d_apsoa = nullptr;     // active lists' interleaved primitive arrays (SoA)
+    PrimSoA apsoa{};
+    std::vector<GPrim> hprims;     // host copy, all-pairs order
     GPair* d_pairs[NPT] = {};
     double* d_schw[NPT] = {};
     GPair* d_apairs[NPT] = {};
@@ -371,7 +375,7 @@ int run_staged_diag(hfgpu_handle* h, int t, int mode, const double* P, double th
         a.cap = n;
         a.bra = h->d_pairs[t];
         a.ket = h->d_pairs[t];
-        a.prims = h->d_prims;
+        a.prims = h->psoa;
         a.boys = h->d_boys;
         a.boysf = h->d_boysf;
         a.acc = h->d_dscratch;
@@ -412,7 +416,7 @@ int launch_diag(hfgpu_handle* h, int mode, const double* P, double thr, double* 
             if (rc) return rc;
             continue;
         }
-        DiagArgs a{h->d_pairs[t], n, h->d_prims, h->d_boys, h->d_schw[t], md ? md : h->d_md, h->nsh, P,
+        DiagArgs a{h->d_pairs[t], n, h->psoa, h->d_boys, h->d_schw[t], md ? md : h->d_md, h->nsh, P,
                    G ? G : h->d_G, h->nb, thr};
         const ClassKernels& K = CLASS_KERNELS[class_index(t, t)];
         diag_kernel(t, mode)<<<(n + K.dg_ppb - 1) / K.dg_ppb, K.dg_threads, 0, h->stream>>>(a);
@@ -444,6 +448,10 @@ int build_active(hfgpu_handle* h) {
     HF_CHECK(cudaStreamSynchronize(h->stream));
     h->last_ref.assign(10, 0);
     long long total_q = 0;
+    std::vector<GPrim> aprims;
+    std::vector<GPair> aps[NPT];
+    std::vector<int2> ashs[NPT];
+    std::vector<double> ascs[NPT];
     for (int t = 0; t < NPT; ++t) {
         const int n = (int)h->pairs[t].size();
         // reference list order is refpos; pairs[t] is stored in that order
@@ -479,14 +487,46 @@ int build_active(hfgpu_handle* h) {
         h->nact[t] = last;
         h->act_np[t].resize(last);
         for (int i = 0; i < last; ++i) h->act_np[t][i] = ap[i].np;
-        if (last) {
-            HF_CHECK(cudaMemcpyAsync(h->d_apairs[t], ap.data(), last * sizeof(GPair), cudaMemcpyHostToDevice,
-                                     h->stream));
-            HF_CHECK(cudaMemcpyAsync(h->d_ash[t], ash.data(), last * sizeof(int2), cudaMemcpyHostToDevice, h->stream));
-            HF_CHECK(cudaMemcpyAsync(h->d_aschw[t], asc.data(), last * sizeof(double), cudaMemcpyHostToDevice,
-                                     h->stream));
-            HF_CHECK(cudaStreamSynchronize(h->stream));
+        // interleave the primitives of equal-count neighbours: entry ik of
+        // pair i of a group [g0, g0+ng) goes to base + ik*ng + (i - g0)
+        for (int i = 0; i < last;) {
+            int j = i + 1;
+            while (j < last && ap[j].np == ap[i].np) ++j;
+            const int ng = j - i, np = ap[i].np;
+            const size_t base = aprims.size();
+            aprims.resize(base + (size_t)np * ng);
+            for (int k = i; k < j; ++k) {
+                for (int ik = 0; ik < np; ++ik) aprims[base + (size_t)ik * ng + (k - i)] = h->hprims[ap[k].p0 + ik];
+                ap[k].p0 = (int)(base + (k - i));
+                ap[k].ps = ng;
+            }
+            i = j;
         }
+        aps[t] = std::move(ap);
+        ashs[t] = std::move(ash);
+        ascs[t] = std::move(asc);
+    }
+    {
+        std::vector<double> soa = prims_soa(aprims);
+        if (h->d_apsoa) cudaFree(h->d_apsoa);
+        h->d_apsoa = nullptr;
+        int rc = dalloc(&h->d_apsoa, std::max<size_t>(soa.size(), 1));
+        if (rc) return rc;
+        h->apsoa = soa_view(h->d_apsoa, aprims.size());
+        if (!soa.empty())
+            HF_CHECK(cudaMemcpyAsync(h->d_apsoa, soa.data(), soa.size() * sizeof(double), cudaMemcpyHostToDevice,
+                                     h->stream));
+        for (int t = 0; t < NPT; ++t) {
+            const int last = h->nact[t];
+            if (!last) continue;
+            HF_CHECK(cudaMemcpyAsync(h->d_apairs[t], aps[t].data(), last * sizeof(GPair), cudaMemcpyHostToDevice,
+                                     h->stream));
+            HF_CHECK(cudaMemcpyAsync(h->d_ash[t], ashs[t].data(), last * sizeof(int2), cudaMemcpyHostToDevice,
+                                     h->stream));
+            HF_CHECK(cudaMemcpyAsync(h->d_aschw[t], ascs[t].data(), last * sizeof(double), cudaMemcpyHostToDevice,
+                                     h->stream));
+        }
+        HF_CHECK(cudaStreamSynchronize(h->stream));
     }
     // screening sub-classes: primitive-count groups of the active lists
     std::vector<std::pair<int, int>> groups[NPT];  // (start, length)
@@ -588,7 +628,7 @@ int run_staged(hfgpu_handle* h, int c, int prec, long long n, const double* P, d
         a.cap = n;
         a.bra = h->d_apairs[K.bi];
         a.ket = h->d_apairs[K.ki];
-        a.prims = h->d_prims;
+        a.prims = h->apsoa;
         a.boys = h->d_boys;
         a.boysf = h->d_boysf;
         a.acc = h->d_scratch;
@@ -695,7 +735,7 @@ int run_non_diag(hfgpu_handle* h, const double* P, double thr, int jonly, double
             if (h->timing) HF_CHECK(cudaEventRecord(h->ev[2 * c], h->stream));
             if (K.mode == 0) {
                 NDArgs a{h->d_q + h->coff[c] + (prec ? h->n64[c] : 0), (int)n, 0, n, h->d_apairs[K.bi],
-                         h->d_apairs[K.ki], h->d_prims, h->d_boys, h->d_boysf, P, h->d_G, h->nb, thr, jonly,
+                         h->d_apairs[K.ki], h->apsoa, h->d_boys, h->d_boysf, P, h->d_G, h->nb, thr, jonly,
                          h->d_stats + c};
                 long long blocks = (n + K.nd_qpb - 1) / K.nd_qpb;
                 (prec ? K.nd32 : K.nd64)<<<(int)blocks, K.nd_threads, 0, h->stream>>>(a);
@@ -769,7 +809,7 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
     const size_t nb2 = (size_t)h->nb * h->nb;
     rc |= dalloc(&h->d_shtyp, h->nsh);
     rc |= dalloc(&h->d_aosh, h->nsh);
-    rc |= dalloc(&h->d_prims, prims.size());
+    rc |= dalloc(&h->d_psoa, 7 * std::max<size_t>(prims.size(), 1));
     rc |= dalloc(&h->d_boys, bt.size());
     rc |= dalloc(&h->d_boysf, btf.size());
     rc |= dalloc(&h->d_P, nb2);
@@ -797,7 +837,12 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
     };
     ce = up(h->d_shtyp, h->shtyp.data(), h->nsh * sizeof(int));
     if (ce == cudaSuccess) ce = up(h->d_aosh, h->aosh.data(), h->nsh * sizeof(int));
-    if (ce == cudaSuccess) ce = up(h->d_prims, prims.data(), prims.size() * sizeof(GPrim));
+    if (ce == cudaSuccess) {
+        std::vector<double> soa = prims_soa(prims);
+        ce = up(h->d_psoa, soa.data(), soa.size() * sizeof(double));
+        h->psoa = soa_view(h->d_psoa, prims.size());
+    }
+    h->hprims = prims;
     if (ce == cudaSuccess) ce = up(h->d_boys, bt.data(), bt.size() * sizeof(double));
     if (ce == cudaSuccess) ce = up(h->d_boysf, btf.data(), btf.size() * sizeof(float));
     for (int t = 0; t < NPT && ce == cudaSuccess; ++t) {
@@ -848,7 +893,7 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
 int hfgpu_finalize(hfgpu_handle* h) {
     if (!h) return HFGPU_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
-    void* bufs[] = {h->d_shtyp, h->d_aosh, h->d_prims, h->d_boys, h->d_boysf, h->d_P, h->d_F, h->d_G,
+    void* bufs[] = {h->d_shtyp, h->d_aosh, h->d_psoa, h->d_apsoa, h->d_boys, h->d_boysf, h->d_P, h->d_F, h->d_G,
                     h->d_md, h->d_subs, h->d_q, h->d_cnt, h->d_stats, h->d_scratch, h->d_dscratch};
     for (void* b : bufs)
         if (b) cudaFree(b);

@@ -57,6 +57,8 @@ inline GPair make_pair(const hfgpu_basis* B, int a, int b, std::vector<GPrim>& p
     g.aoa = B->aosh[a];
     g.aob = B->aosh[b];
     g.p0 = (int)prims.size();
+    g.ps = 1;
+    g.pad = 0;
     double r2ab = 0;
     for (int x = 0; x < 3; ++x) r2ab += (g.A[x] - g.B[x]) * (g.A[x] - g.B[x]);
     for (int za = 0; za < B->nzet[a]; ++za)
@@ -127,6 +129,27 @@ inline void build_boys_table(std::vector<double>& bt, std::vector<float>& btf) {
                 btf[i] = (float)v;
             }
         }
+}
+
+// Structure-of-arrays copy of primitive pairs: 7 arrays of n doubles
+// (p, Px, Py, Pz, K, w1, w2) back to back.
+inline std::vector<double> prims_soa(const std::vector<GPrim>& prims) {
+    const size_t n = prims.size();
+    std::vector<double> s(7 * n);
+    for (size_t i = 0; i < n; ++i) {
+        s[i] = prims[i].p;
+        s[n + i] = prims[i].P[0];
+        s[2 * n + i] = prims[i].P[1];
+        s[3 * n + i] = prims[i].P[2];
+        s[4 * n + i] = prims[i].K;
+        s[5 * n + i] = prims[i].w1;
+        s[6 * n + i] = prims[i].w2;
+    }
+    return s;
+}
+
+inline PrimSoA soa_view(const double* base, size_t n) {
+    return PrimSoA{base, base + n, base + 2 * n, base + 3 * n, base + 4 * n, base + 5 * n, base + 6 * n};
 }
 
 }  // namespace hfgpu

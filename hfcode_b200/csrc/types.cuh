@@ -26,14 +26,43 @@ struct GPrim {
     double pad;
 };
 
-// Shell pair in GPU orientation (larger shell first).
+// Shell pair in GPU orientation (larger shell first).  Primitive ib of the
+// pair is entry p0 + ib * ps of the primitive-pair arrays: ps = 1 for the
+// all-pairs layout, and ps = group size for the active lists, whose pairs of
+// equal primitive count are interleaved so that the lanes of a warp, working
+// on neighbouring pairs, read neighbouring addresses.
 struct GPair {
     double A[3];
     double B[3];
-    int p0, np;    // range in the primitive-pair array
+    int p0, np;    // first primitive and primitive count
     int sa, sb;    // shell indices
     int aoa, aob;  // first AO of each shell
+    int ps, pad;   // primitive stride
 };
+
+// Primitive pairs as structure of arrays (fields of GPrim).
+struct PrimSoA {
+    const double* p;
+    const double* x;
+    const double* y;
+    const double* z;
+    const double* K;
+    const double* w1;
+    const double* w2;
+};
+
+__device__ __forceinline__ GPrim load_prim(const PrimSoA& s, int i) {
+    GPrim g;
+    g.p = __ldg(s.p + i);
+    g.P[0] = __ldg(s.x + i);
+    g.P[1] = __ldg(s.y + i);
+    g.P[2] = __ldg(s.z + i);
+    g.K = __ldg(s.K + i);
+    g.w1 = __ldg(s.w1 + i);
+    g.w2 = __ldg(s.w2 + i);
+    g.pad = 0.0;
+    return g;
+}
 
 // ---------------------------------------------------------------- Boys ----
 // F_m(T) for m = 0..M.  T > 28: F_0 = sqrt(pi/T)/2 and upward recursion

@@ -52,9 +52,11 @@ int hc_eri(void* hh, int cls, int L, int a, int b, int c, int d, int f32, double
     std::vector<GPrim> prims;
     GPair bra = make_pair(h->B, a, b, prims);
     GPair ket = make_pair(h->B, c, d, prims);
+    std::vector<double> soa = prims_soa(prims);
+    const PrimSoA ps = soa_view(soa.data(), prims.size());
     const double* t = h->bt.data() + (size_t)L * BOYS_NPT * BOYS_K;
     const float* tf = h->btf.data() + (size_t)L * BOYS_NPT * BOYS_K;
-    HOST_ERI[cls](bra, ket, prims.data(), t, tf, out, f32);
+    HOST_ERI[cls](bra, ket, ps, t, tf, out, f32);
     return 0;
 }
 
