@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--density", default="huckel", choices=["huckel", "guess"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the FP64-vs-mixed SCF study")
+    ap.add_argument("--mixed-cutoffs", default="1e-7,1e-5")
     return ap.parse_args()
 
 
@@ -145,6 +147,74 @@ def cpu_baseline(sh, p, target_s: float, n_pass_total: int):
             "sample": f"bra rows ii % {stride} == 0 of every class block: {n} of {n_pass_total} screened-in "
                       f"quartets in {dt:.1f} s, extrapolated by quartet count; diag part timed in full "
                       f"({t_diag:.2f} s)"}
+
+
+def mixed_study(fock, mol, sh, cutoffs, dev):
+    """FP64 vs mixed precision on the SCF path: converged energies of the
+    reference protocol (conve 1e-9) with FP64 and with mixed incremental
+    builds, and the speed of one incremental (delta-P) build near
+    convergence in both forms, with max|dF| between them."""
+    import torch
+    from hfcode_b200 import basis, onee, scf
+    bas = basis.load_basis("6-31G(d)")
+    p0 = basis.density_superposition(mol, bas, sh.nb)
+    ints = onee.one_electron(mol, sh)
+    out = {"cutoffs": {}}
+    fb = fock.FockBuilder(sh)
+    t0 = time.perf_counter()
+    dens = []
+
+    def keep(h):
+        pass
+
+    r64 = scf.direct_hartreefock(mol, sh, fb, p_guess=p0, conve=1e-9, conv=1e-6, maxiter=80, ints=ints)
+    out["scf_fp64"] = {"energy": r64.energy, "cycles": r64.cycles, "converged": r64.converged,
+                       "seconds": time.perf_counter() - t0}
+    # a delta-P near convergence: the converged density against the core-free
+    # one-cycle update (P_next - P), the size the incremental builds see late
+    nb = sh.nb
+    f = r64.F
+    X = onee.s_minus_half(ints[0])
+    _, C = np.linalg.eigh(X @ f @ X.T)
+    C = X @ C
+    p_next = 2.0 * C[:, :mol.nocc] @ C[:, :mol.nocc].T
+    dp = p_next - r64.P
+    out["delta_p_max"] = float(np.max(np.abs(dp)))
+    P = torch.from_numpy(np.ascontiguousarray(dp)).to(dev)
+    F = torch.zeros((nb, nb), dtype=torch.float64, device=dev)
+    stream = torch.cuda.ExternalStream(fb.stream(), device=dev)
+
+    def timed(cut, reps=3):
+        ts = []
+        for _ in range(reps + 1):
+            F.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fb.fock_build_device(F.data_ptr(), P.data_ptr(), THR, THR * 0.1, cut)
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts[1:])), F.cpu().numpy().copy(), fb.class_stats()
+
+    t64, f64, st64 = timed(0.0)
+    out["delta_build_ms_fp64"] = t64
+    for cut in cutoffs:
+        tm, fm, stm = timed(cut)
+        fbm = fock.FockBuilder(sh)
+        t1 = time.perf_counter()
+        rm = scf.direct_hartreefock(mol, sh, fbm, p_guess=p0, conve=1e-9, conv=1e-6, maxiter=80, ints=ints,
+                                    fp32_cutoff=cut)
+        fbm.close()
+        out["cutoffs"][f"{cut:g}"] = {
+            "delta_build_ms": tm, "speedup_vs_fp64": t64 / tm,
+            "fp32_quartet_fraction": float(stm["fp32"].sum() / max(1, stm["scattered"].sum())),
+            "max_abs_dF_vs_fp64": float(np.max(np.abs(fm - f64))),
+            "scf_energy": rm.energy, "abs_dE_vs_fp64": abs(rm.energy - r64.energy), "scf_cycles": rm.cycles,
+            "converged": rm.converged, "scf_seconds": time.perf_counter() - t1}
+    fb.close()
+    return out
 
 
 def run_reference(args):
@@ -291,6 +361,8 @@ def main():
            "e2e": e2e, "gpu_launches": launches_per_step * args.steps, "roofline": roof,
            "fp64_peak_tflops": peak_tf, "fp32_peak_tflops": fp32_peak / 1e3,
            "clocks": clk.summary()}
+    if rank == 0 and world == 1 and not args.no_mixed:
+        out["mixed"] = mixed_study(fock, mol, sh, [float(x) for x in args.mixed_cutoffs.split(",")], dev)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(sh, p, args.cpu_seconds, n_pass)
     if rank == 0:
