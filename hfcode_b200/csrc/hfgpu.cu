@@ -66,6 +66,7 @@ thread_local std::string g_err;
     } while (0)
 
 constexpr double SHTHRESH = 1e-11;      // molprops.f90:163
+constexpr int NSTREAM = 4;              // concurrent class streams of the off-diagonal build
 // bra and ket pair types of the 21 quartet classes (pair types i <= j, row by row)
 __constant__ int CLS_BI[NCLS] = {0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 1, 2, 2, 2, 2, 3, 3, 3, 4, 4, 5};
 __constant__ int CLS_KI[NCLS] = {0, 1, 2, 3, 4, 5, 1, 2, 3, 4, 5, 2, 3, 4, 5, 3, 4, 5, 4, 5, 5};
@@ -234,6 +235,8 @@ struct hfgpu_handle {
     bool have_schwarz = false;
     int timing = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t aux[NSTREAM] = {};    // independent classes run concurrently on these
+    cudaEvent_t fork = nullptr, join[NSTREAM] = {};
     // device
     int* d_shtyp = nullptr;
     int* d_aosh = nullptr;
@@ -266,6 +269,7 @@ struct hfgpu_handle {
     size_t dstride[NPT] = {};
     size_t scratch_doubles = 0;
     size_t stride[NCLS] = {};      // quartets per chunk of each staged class
+    size_t slot_doubles = 0;       // scratch per class stream
     unsigned long long* d_cnt = nullptr;
     ClassStats* d_stats = nullptr;
     // last build statistics
@@ -425,10 +429,10 @@ int launch_diag(hfgpu_handle* h, int mode, const double* P, double thr, double* 
     return HFGPU_OK;
 }
 
-// Scratch budget of the staged classes in doubles (default 3 GiB; the
+// Scratch budget of the staged classes in doubles (default 6 GiB; the
 // HFGPU_SCRATCH_MB environment variable overrides it).
 size_t scratch_budget_doubles() {
-    size_t mb = 3072;
+    size_t mb = 6144;
     if (const char* e = getenv("HFGPU_SCRATCH_MB")) {
         long v = atol(e);
         if (v > 0) mb = (size_t)v;
@@ -590,7 +594,7 @@ int build_active(hfgpu_handle* h) {
     // scratch of the staged classes: one chunk of stride quartets holds
     // (accumulators + outputs + role maxima) doubles per quartet
     size_t need = 0;
-    const size_t budget = scratch_budget_doubles();
+    const size_t budget = scratch_budget_doubles() / NSTREAM;  // one slot per class stream
     for (int c = 0; c < NCLS; ++c) {
         const ClassKernels& K = CLASS_KERNELS[c];
         h->stride[c] = 0;
@@ -601,21 +605,23 @@ int build_active(hfgpu_handle* h) {
         h->stride[c] = st;
         need = std::max(need, st * per);
     }
-    if (need > h->scratch_doubles) {
+    if (need * NSTREAM > h->scratch_doubles) {
         if (h->d_scratch) cudaFree(h->d_scratch);
         h->d_scratch = nullptr;
         h->scratch_doubles = 0;
-        int rc = dalloc(&h->d_scratch, need);
+        int rc = dalloc(&h->d_scratch, need * NSTREAM);
         if (rc) return rc;
-        h->scratch_doubles = need;
+        h->scratch_doubles = need * NSTREAM;
     }
+    h->slot_doubles = need;
     h->have_schwarz = true;
     return HFGPU_OK;
 }
 
 // Staged class: chunks of the quartet list through the accumulator roles
 // (mode 2), the output roles and the scatter kernel.
-int run_staged(hfgpu_handle* h, int c, int prec, long long n, const double* P, double thr, int jonly) {
+int run_staged(hfgpu_handle* h, int c, int prec, long long n, const double* P, double thr, int jonly,
+               cudaStream_t stream, double* scratch) {
     const ClassKernels& K = CLASS_KERNELS[c];
     const size_t st = h->stride[c];
     for (long long q0 = 0; q0 < n; q0 += (long long)st) {
@@ -631,9 +637,9 @@ int run_staged(hfgpu_handle* h, int c, int prec, long long n, const double* P, d
         a.prims = h->apsoa;
         a.boys = h->d_boys;
         a.boysf = h->d_boysf;
-        a.acc = h->d_scratch;
-        a.out = h->d_scratch + (size_t)K.nacc * st;
-        a.mx = h->d_scratch + (size_t)(K.nacc + K.nout) * st;
+        a.acc = scratch;
+        a.out = scratch + (size_t)K.nacc * st;
+        a.mx = scratch + (size_t)(K.nacc + K.nout) * st;
         a.stride = st;
         a.nroles = K.nrole_b;
         a.P = P;
@@ -645,14 +651,14 @@ int run_staged(hfgpu_handle* h, int c, int prec, long long n, const double* P, d
         a.stats = h->d_stats + c;
         const int blocks = (m + ND_THREADS - 1) / ND_THREADS;
         for (int r = 0; r < K.nrole_a; ++r) {
-            (prec ? K.sa32[r] : K.sa64[r])<<<blocks, ND_THREADS, 0, h->stream>>>(a);
+            (prec ? K.sa32[r] : K.sa64[r])<<<blocks, ND_THREADS, 0, stream>>>(a);
             HF_CHECK(cudaGetLastError());
         }
         for (int r = 0; r < K.nrole_b; ++r) {
-            (prec ? K.sb32[r] : K.sb64[r])<<<blocks, ND_THREADS, 0, h->stream>>>(a);
+            (prec ? K.sb32[r] : K.sb64[r])<<<blocks, ND_THREADS, 0, stream>>>(a);
             HF_CHECK(cudaGetLastError());
         }
-        K.scat<<<blocks, ND_THREADS, 0, h->stream>>>(a);
+        K.scat<<<blocks, ND_THREADS, 0, stream>>>(a);
         HF_CHECK(cudaGetLastError());
     }
     return HFGPU_OK;
@@ -725,32 +731,60 @@ int run_non_diag(hfgpu_handle* h, const double* P, double thr, int jonly, double
         cnt[2 * c] = (unsigned long long)h->n64[c];
         cnt[2 * c + 1] = (unsigned long long)h->n32[c];
     }
+    // work items (class, precision) over NSTREAM concurrent streams, largest
+    // first onto the least-loaded stream; with timing on, everything runs in
+    // order on the handle's stream
+    struct Item { int c, prec; long long n; double w; };
+    std::vector<Item> items;
     for (int c = 0; c < NCLS; ++c) {
-        const ClassKernels& K = CLASS_KERNELS[c];
         h->st_pass[c] = (long long)(cnt[2 * c] + cnt[2 * c + 1]);
         h->st_ms[c] = 0.0;
         for (int prec = 0; prec < 2; ++prec) {
-            long long n = (long long)cnt[2 * c + prec];
-            if (n == 0) continue;
-            if (h->timing) HF_CHECK(cudaEventRecord(h->ev[2 * c], h->stream));
-            if (K.mode == 0) {
-                NDArgs a{h->d_q + h->coff[c] + (prec ? h->n64[c] : 0), (int)n, 0, n, h->d_apairs[K.bi],
-                         h->d_apairs[K.ki], h->apsoa, h->d_boys, h->d_boysf, P, h->d_G, h->nb, thr, jonly,
-                         h->d_stats + c};
-                long long blocks = (n + K.nd_qpb - 1) / K.nd_qpb;
-                (prec ? K.nd32 : K.nd64)<<<(int)blocks, K.nd_threads, 0, h->stream>>>(a);
-                HF_CHECK(cudaGetLastError());
-            } else {
-                int rc = run_staged(h, c, prec, n, P, thr, jonly);
-                if (rc) return rc;
-            }
-            if (h->timing) {
-                HF_CHECK(cudaEventRecord(h->ev[2 * c + 1], h->stream));
-                HF_CHECK(cudaEventSynchronize(h->ev[2 * c + 1]));
-                float ms = 0;
-                cudaEventElapsedTime(&ms, h->ev[2 * c], h->ev[2 * c + 1]);
-                h->st_ms[c] += ms;
-            }
+            const long long n = (long long)cnt[2 * c + prec];
+            if (n > 0) items.push_back({c, prec, n, (double)n * CLASS_KERNELS[c].nout});
+        }
+    }
+    const bool multi = !h->timing;
+    if (multi) {
+        std::stable_sort(items.begin(), items.end(), [](const Item& x, const Item& y) { return x.w > y.w; });
+        HF_CHECK(cudaEventRecord(h->fork, h->stream));
+        for (int k = 0; k < NSTREAM; ++k) HF_CHECK(cudaStreamWaitEvent(h->aux[k], h->fork, 0));
+    }
+    double load[NSTREAM] = {};
+    for (const Item& it : items) {
+        const int c = it.c, prec = it.prec;
+        const long long n = it.n;
+        const ClassKernels& K = CLASS_KERNELS[c];
+        int k = 0;
+        for (int q = 1; q < NSTREAM; ++q)
+            if (load[q] < load[k]) k = q;
+        load[k] += it.w;
+        cudaStream_t st = multi ? h->aux[k] : h->stream;
+        double* slot = h->d_scratch ? h->d_scratch + (multi ? (size_t)k * h->slot_doubles : 0) : nullptr;
+        if (h->timing) HF_CHECK(cudaEventRecord(h->ev[2 * c], h->stream));
+        if (K.mode == 0) {
+            NDArgs a{h->d_q + h->coff[c] + (prec ? h->n64[c] : 0), (int)n, 0, n, h->d_apairs[K.bi],
+                     h->d_apairs[K.ki], h->apsoa, h->d_boys, h->d_boysf, P, h->d_G, h->nb, thr, jonly,
+                     h->d_stats + c};
+            long long blocks = (n + K.nd_qpb - 1) / K.nd_qpb;
+            (prec ? K.nd32 : K.nd64)<<<(int)blocks, K.nd_threads, 0, st>>>(a);
+            HF_CHECK(cudaGetLastError());
+        } else {
+            int rc = run_staged(h, c, prec, n, P, thr, jonly, st, slot);
+            if (rc) return rc;
+        }
+        if (h->timing) {
+            HF_CHECK(cudaEventRecord(h->ev[2 * c + 1], h->stream));
+            HF_CHECK(cudaEventSynchronize(h->ev[2 * c + 1]));
+            float ms = 0;
+            cudaEventElapsedTime(&ms, h->ev[2 * c], h->ev[2 * c + 1]);
+            h->st_ms[c] += ms;
+        }
+    }
+    if (multi) {
+        for (int k = 0; k < NSTREAM; ++k) {
+            HF_CHECK(cudaEventRecord(h->join[k], h->aux[k]));
+            HF_CHECK(cudaStreamWaitEvent(h->stream, h->join[k], 0));
         }
     }
     ClassStats st[NCLS];
@@ -831,6 +865,11 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
         return HFGPU_ERR_NOMEM;
     }
     for (int i = 0; i < 2 * NCLS + 2; ++i) cudaEventCreate(&h->ev[i]);
+    cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming);
+    for (int k = 0; k < NSTREAM; ++k) {
+        cudaStreamCreateWithFlags(&h->aux[k], cudaStreamNonBlocking);
+        cudaEventCreateWithFlags(&h->join[k], cudaEventDisableTiming);
+    }
     auto up = [&](void* d, const void* s, size_t bytes) {
         if (bytes == 0) return cudaSuccess;
         return cudaMemcpy(d, s, bytes, cudaMemcpyHostToDevice);
@@ -904,6 +943,14 @@ int hfgpu_finalize(hfgpu_handle* h) {
     }
     for (int i = 0; i < 2 * NCLS + 2; ++i)
         if (h->ev[i]) cudaEventDestroy(h->ev[i]);
+    for (int k = 0; k < NSTREAM; ++k) {
+        if (h->aux[k]) {
+            cudaStreamSynchronize(h->aux[k]);
+            cudaStreamDestroy(h->aux[k]);
+        }
+        if (h->join[k]) cudaEventDestroy(h->join[k]);
+    }
+    if (h->fork) cudaEventDestroy(h->fork);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return HFGPU_OK;
