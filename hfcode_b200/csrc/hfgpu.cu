@@ -270,6 +270,8 @@ struct hfgpu_handle {
     size_t scratch_doubles = 0;
     size_t stride[NCLS] = {};      // quartets per chunk of each staged class
     size_t slot_doubles = 0;       // scratch per class stream
+    size_t scratch_budget = 0;     // bytes; 0 = default (HFGPU_SCRATCH_MB or 6 GiB)
+    size_t naprims = 0;            // primitive pairs of the active lists
     unsigned long long* d_cnt = nullptr;
     ClassStats* d_stats = nullptr;
     // last build statistics
@@ -517,6 +519,7 @@ int build_active(hfgpu_handle* h) {
         int rc = dalloc(&h->d_apsoa, std::max<size_t>(soa.size(), 1));
         if (rc) return rc;
         h->apsoa = soa_view(h->d_apsoa, aprims.size());
+        h->naprims = aprims.size();
         if (!soa.empty())
             HF_CHECK(cudaMemcpyAsync(h->d_apsoa, soa.data(), soa.size() * sizeof(double), cudaMemcpyHostToDevice,
                                      h->stream));
@@ -594,7 +597,8 @@ int build_active(hfgpu_handle* h) {
     // scratch of the staged classes: one chunk of stride quartets holds
     // (accumulators + outputs + role maxima) doubles per quartet
     size_t need = 0;
-    const size_t budget = scratch_budget_doubles() / NSTREAM;  // one slot per class stream
+    const size_t budget = (h->scratch_budget ? h->scratch_budget / sizeof(double) : scratch_budget_doubles()) /
+                          NSTREAM;  // one slot per class stream
     for (int c = 0; c < NCLS; ++c) {
         const ClassKernels& K = CLASS_KERNELS[c];
         h->stride[c] = 0;
@@ -1016,6 +1020,34 @@ int hfgpu_fock_build_device(hfgpu_handle* h, double* f_dev, const double* p_dev,
     if ((rc = launch_diag(h, 1, p_dev, thr_diag))) return rc;
     if ((rc = run_non_diag(h, p_dev, thr_non_diag, 0, fp32_cutoff))) return rc;
     return launch_symm(h, f_dev);
+}
+
+int hfgpu_set_scratch_budget(hfgpu_handle* h, size_t bytes) {
+    if (!h) return set_err(HFGPU_ERR_ARG, "null handle");
+    if (h->have_schwarz) return set_err(HFGPU_ERR_STATE, "set the scratch budget before fock_build_initial_diag");
+    h->scratch_budget = bytes;
+    return HFGPU_OK;
+}
+
+int hfgpu_device_bytes(const hfgpu_handle* h, size_t* bytes) {
+    if (!h || !bytes) return set_err(HFGPU_ERR_ARG, "null argument");
+    size_t b = 0;
+    const size_t nb2 = (size_t)h->nb * h->nb;
+    b += 3 * nb2 * sizeof(double);                            // P, F, G
+    b += (size_t)h->nsh * h->nsh * sizeof(double);            // maxdm
+    b += 2 * (size_t)h->nsh * sizeof(int);
+    b += 7 * h->hprims.size() * sizeof(double);               // all-pairs primitives
+    for (int t = 0; t < NPT; ++t) {
+        const size_t n = h->pairs[t].size();
+        b += n * (2 * sizeof(GPair) + sizeof(double) * 2 + sizeof(int2) + (h->d_diaglist[t] ? sizeof(uint2) : 0));
+    }
+    b += 7 * h->naprims * sizeof(double);                     // active-list primitives
+    b += h->qcap * sizeof(uint2);                             // quartet lists
+    b += h->scratch_doubles * sizeof(double);                 // staged scratch
+    b += h->subcap * (sizeof(ScreenSub) + 2 * sizeof(unsigned long long));
+    b += (size_t)(BOYS_MMAX + 1) * BOYS_NPT * BOYS_K * (sizeof(double) + sizeof(float));
+    *bytes = b;
+    return HFGPU_OK;
 }
 
 int hfgpu_dims(const hfgpu_handle* h, int* nb, int* nsh, int* npairs) {

@@ -60,6 +60,8 @@ def _load():
     lib.hfgpu_last_error.restype = ctypes.c_char_p
     lib.hfgpu_measure_fma_peak.argtypes = [d, d]
     lib.hfgpu_fock_build_diag_static.argtypes = [vp, vp, vp, ctypes.c_double]
+    lib.hfgpu_set_scratch_budget.argtypes = [vp, ctypes.c_size_t]
+    lib.hfgpu_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
     return lib
 
 
@@ -70,7 +72,8 @@ EXPORTS = ["hfgpu_init", "hfgpu_fock_build_initial_diag", "hfgpu_fock_build_diag
            "hfgpu_fock_build_non_diag_mixed", "hfgpu_fock_build_device", "hfgpu_dims",
            "hfgpu_get_schwarz", "hfgpu_get_class_stats", "hfgpu_set_timing", "hfgpu_stream",
            "hfgpu_finalize", "hfgpu_last_error", "hfgpu_measure_fma_peak",
-           "hfgpu_fock_build_diag_static", "hfgpu_one_electron"]
+           "hfgpu_fock_build_diag_static", "hfgpu_one_electron", "hfgpu_set_scratch_budget",
+           "hfgpu_device_bytes"]
 
 
 def measure_fma_peak():
@@ -97,7 +100,7 @@ def _dp(a: np.ndarray):
 class FockBuilder:
     """One SCF instance's resident Fock-build state on the current GPU."""
 
-    def __init__(self, shells: ShellSet):
+    def __init__(self, shells: ShellSet, scratch_budget: Optional[int] = None):
         self.shells = shells
         self.nb = shells.nb
         self.nsh = shells.nsh
@@ -105,6 +108,8 @@ class FockBuilder:
         h = ctypes.c_void_p()
         _check(_lib.hfgpu_init(ctypes.addressof(self._desc.struct), ctypes.byref(h)), "hfgpu_init")
         self.h = h
+        if scratch_budget is not None:
+            self.set_scratch_budget(scratch_budget)
 
     def close(self):
         if getattr(self, "h", None):
@@ -160,6 +165,14 @@ class FockBuilder:
         scratch (no device allocation; see include/hfgpu.h)."""
         _check(_lib.hfgpu_fock_build_diag_static(self.h, ctypes.c_void_p(f_ptr), ctypes.c_void_p(p_ptr),
                                                  float(thr)), "fock_build_diag_static")
+
+    def set_scratch_budget(self, nbytes: int):
+        _check(_lib.hfgpu_set_scratch_budget(self.h, int(nbytes)), "set_scratch_budget")
+
+    def device_bytes(self) -> int:
+        b = ctypes.c_size_t()
+        _check(_lib.hfgpu_device_bytes(self.h, ctypes.byref(b)), "device_bytes")
+        return int(b.value)
 
     def stream(self) -> int:
         return int(_lib.hfgpu_stream(self.h) or 0)

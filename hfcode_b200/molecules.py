@@ -113,32 +113,37 @@ def c60(r66: float = 1.40, r56: float = 1.45) -> Molecule:
     return Molecule(["C"] * 60, xyz)
 
 
-def water_cluster(k: int, rng: np.random.Generator, min_oo: float = 2.7,
-                  box_per_mol: float = 3.1) -> Molecule:
-    """k rigid waters at random seeded orientations and positions in a cube
-    sized for ~box_per_mol A per molecule, O-O >= min_oo A (rejection)."""
+def water_cluster(k: int, rng: np.random.Generator, min_oo: float = 2.7, min_atom: float = 1.5,
+                  box_per_mol: float = 3.3) -> Molecule:
+    """k rigid waters at seeded random positions and orientations in a cube
+    of ~box_per_mol A per molecule: O-O >= min_oo A by rejection sampling,
+    and no two atoms of different waters closer than min_atom A."""
     mono = water().coords_ang
     side = box_per_mol * max(1.0, k ** (1.0 / 3.0))
-    centers: List[np.ndarray] = []
-    labels: List[str] = []
-    xyz = []
+    placed: List[np.ndarray] = []  # (3, 3) coordinates per water
     tries = 0
-    while len(centers) < k:
+    while len(placed) < k:
         tries += 1
         if tries > 200000:
             raise RuntimeError("could not place waters")
-        c = rng.uniform(0.0, side, size=3) if centers else np.zeros(3)
-        if any(np.linalg.norm(c - o) < min_oo for o in centers):
-            continue
-        q = rng.normal(size=4); q /= np.linalg.norm(q)
+        c = rng.uniform(0.0, side, size=3) if placed else np.zeros(3)
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
         w, x, y, z = q
         rot = np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
                         [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
                         [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
-        centers.append(c)
-        for lab, r in zip(["O", "H", "H"], mono):
-            labels.append(lab); xyz.append(c + rot @ r)
-    return Molecule(labels, np.array(xyz))
+        xyz = c + mono @ rot.T
+        ok = True
+        for other in placed:
+            if np.linalg.norm(xyz[0] - other[0]) < min_oo or \
+                    np.min(np.linalg.norm(xyz[:, None] - other[None], axis=-1)) < min_atom:
+                ok = False
+                break
+        if ok:
+            placed.append(xyz)
+    labels = ["O", "H", "H"] * k
+    return Molecule(labels, np.vstack(placed))
 
 
 def by_name(name: str) -> Molecule:
@@ -149,7 +154,7 @@ def by_name(name: str) -> Molecule:
         return benzene()
     if name == "c60":
         return c60()
-    if name.startswith("c") and name.endswith("h") is False and "h" in name:
+    if name.startswith("c") and "h" in name:  # CnH2n+2, e.g. "c20h42"
         n = int(name[1:name.index("h")])
         return alkane(n)
     raise ValueError(name)

@@ -100,6 +100,15 @@ int hfgpu_get_class_stats(const hfgpu_handle* h, long long* n_pass, long long* n
  * kernels. */
 int hfgpu_set_timing(hfgpu_handle* h, int on);
 
+/* Upper bound in bytes of the staged classes' scratch (chunks of quartets
+ * through the accumulator/output roles); set before
+ * hfgpu_fock_build_initial_diag.  Default: HFGPU_SCRATCH_MB or 6 GiB. */
+int hfgpu_set_scratch_budget(hfgpu_handle* h, size_t bytes);
+
+/* Device memory the handle holds, in bytes (pair data, screening tables,
+ * quartet lists, scratch, F/P/G); used for admission by HBM footprint. */
+int hfgpu_device_bytes(const hfgpu_handle* h, size_t* bytes);
+
 /* The CUDA stream the handle enqueues on (a cudaStream_t). */
 void* hfgpu_stream(hfgpu_handle* h);
 
