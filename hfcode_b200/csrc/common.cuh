@@ -154,10 +154,14 @@ struct ClassStats {
 };
 
 struct NDArgs {
-    const uint2* quartets;  // this class's list (fp64 from the front, fp32 from the back)
-    int n;                  // number of quartets to process
-    int from_back;          // 1: entry t is quartets[cap-1-t]
-    long long cap;
+    const uint2* quartets;  // this class's list: FP64 entries, then FP32 entries
+    int n;                  // number of quartets to process (ncls == nullptr)
+    // Device-side counts [2 * NCLS] (FP64, FP32 per class) written by the
+    // screen; when set, the count is ncls[2*cls+prec] and the FP32 entries
+    // start after the class's ncls[2*cls] FP64 entries, so the launch needs
+    // no host round trip and can be captured in a CUDA graph.
+    const unsigned long long* ncls;
+    int cls, prec;
     const GPair* bra;
     const GPair* ket;
     PrimSoA prims;
@@ -205,13 +209,19 @@ __global__ void __launch_bounds__(ND_THREADS) k_nondiag(NDArgs a) {
     static_assert(NA * NB * NC * ND == C::NOUT, "class size");
     unsigned long long nsc = 0, npr = 0;
     const int stride = gridDim.x * blockDim.x;
+    int n = a.n;
+    const uint2* quartets = a.quartets;
+    if (a.ncls) {
+        n = (int)a.ncls[2 * a.cls + a.prec];
+        if (a.prec) quartets += a.ncls[2 * a.cls];
+    }
     // every thread runs the same number of loop trips so the warp-level
     // statistics reduction below sees all 32 lanes
-    const int trips = (a.n + stride - 1) / stride;
+    const int trips = (n + stride - 1) / stride;
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     for (int it = 0; it < trips; ++it, t += stride) {
-        if (t >= a.n) continue;
-        const uint2 q = a.from_back ? a.quartets[a.cap - 1 - t] : a.quartets[t];
+        if (t >= n) continue;
+        const uint2 q = quartets[t];
         const GPair bra = a.bra[q.x];
         const GPair ket = a.ket[q.y];
         Real e[C::NOUT];
@@ -280,10 +290,10 @@ __global__ void __launch_bounds__(ND_THREADS) k_diag(DiagArgs a) {
 // per-role maxima, each [row][stride] with one column per quartet).
 struct StagedArgs {
     const uint2* quartets;
-    int n;                 // quartets in this chunk
+    int n;                 // quartets in this chunk (an upper bound when ncls is set)
     long long q0;          // chunk start within the list
-    int from_back;         // FP32 entries fill the list from the back
-    long long cap;
+    const unsigned long long* ncls;  // device-side counts, as in NDArgs (or nullptr)
+    int cls, prec;
     const GPair* bra;
     const GPair* ket;
     PrimSoA prims;
@@ -307,9 +317,17 @@ struct StagedArgs {
     int nsh;
 };
 
+// Quartets of this chunk: a.n, or with device-side counts the part of the
+// list left after q0, at most a.n.
+__device__ __forceinline__ int staged_count(const StagedArgs& a) {
+    if (!a.ncls) return a.n;
+    const long long left = (long long)a.ncls[2 * a.cls + a.prec] - a.q0;
+    return (int)(left < 0 ? 0 : left < a.n ? left : a.n);
+}
+
 __device__ __forceinline__ uint2 staged_quartet(const StagedArgs& a, int t) {
-    const long long i = a.q0 + t;
-    return a.from_back ? a.quartets[a.cap - 1 - i] : a.quartets[i];
+    const long long i = a.q0 + t + (a.ncls && a.prec ? (long long)a.ncls[2 * a.cls] : 0);
+    return a.quartets[i];
 }
 
 // Post-screen (max |e| over all roles < thr, fock_build_non_diag.f90:69) and
@@ -318,7 +336,7 @@ template <int NA, int NB, int NC, int ND>
 __global__ void __launch_bounds__(ND_THREADS) k_scatter_staged(StagedArgs a) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long nsc = 0, npr = 0;
-    if (t < a.n) {
+    if (t < staged_count(a)) {
         double m = 0.0;
         for (int r = 0; r < a.nroles; ++r) m = fmax(m, a.mx[(size_t)r * a.stride + t]);
         const uint2 q = staged_quartet(a, t);
@@ -342,7 +360,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_scatter_staged(StagedArgs a) {
 template <int NA, int NB, int MODE>
 __global__ void __launch_bounds__(ND_THREADS) k_scatter_diag(StagedArgs a) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= a.n) return;
+    if (t >= staged_count(a)) return;
     const uint2 q = staged_quartet(a, t);
     const GPair pr = a.bra[q.x];
     if (MODE == 0) {

@@ -27,6 +27,7 @@ Run as a script to regenerate ``generated/eri_classes.cuh``.
 from __future__ import annotations
 
 import itertools
+import json
 import math
 import os
 import sys
@@ -561,8 +562,23 @@ ACC_GROUP = 48      # accumulators per stage-A role (d-heavy classes)
 OUT_GROUP3 = 25     # outputs per stage-B role (d-heavy classes)
 MAXR = 64           # role slots in ClassKernels
 
+# Per-class shape overrides (measured on the device; see tuning.json beside
+# this file): {"<tag>": {"acc_max": .., "out_max": .., "max_roles2": ..,
+# "acc_group": .., "out_group3": ..}}.  HFGPU_TUNING names another file.
+_TUNING_FILE = os.environ.get("HFGPU_TUNING") or os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                                                              "tuning.json")
 
-def acc_groups(g: "ClassGen"):
+
+def class_params(tag: str) -> dict:
+    prm = {"acc_max": ACC_MAX, "out_max": OUT_MAX, "max_roles2": MAX_ROLES2, "acc_group": ACC_GROUP,
+           "out_group3": OUT_GROUP3}
+    if os.path.exists(_TUNING_FILE):
+        with open(_TUNING_FILE) as fh:
+            prm.update(json.load(fh).get(tag, {}))
+    return prm
+
+
+def acc_groups(g: "ClassGen", group: int = ACC_GROUP):
     """Partition of all accumulator keys into stage-A roles; the key order
     that minimises the summed VRR terms wins."""
     keys = list(g.all_keys())
@@ -575,7 +591,7 @@ def acc_groups(g: "ClassGen"):
     best = None
     for name, fn in orders.items():
         ks = sorted(keys, key=fn)
-        groups = [ks[i:i + ACC_GROUP] for i in range(0, len(ks), ACC_GROUP)]
+        groups = [ks[i:i + group] for i in range(0, len(ks), group)]
         cost = sum(g._vrr_block(set(gr))[2]["vrr"] for gr in groups)
         if best is None or cost < best[0]:
             best = (cost, groups)
@@ -599,7 +615,8 @@ def class_source(ci: int, bi: int, ki: int):
     g = ClassGen(PAIR_TYPES[bi], PAIR_TYPES[ki], "double")
     g32 = ClassGen(PAIR_TYPES[bi], PAIR_TYPES[ki], "float", suffix="_f32")
     g.flop_model()
-    roles = g.partition(ACC_MAX, OUT_MAX)
+    prm = class_params(g.tag)
+    roles = g.partition(prm["acc_max"], prm["out_max"])
     funcs, kern = [], []
     reg = []
     NA, NB, NC, ND = g.nf
@@ -619,7 +636,7 @@ def class_source(ci: int, bi: int, ki: int):
             reg.append(f"    k->diag0 = k_diag<Cls_{g.tag}, 0>;\n    k->diag1 = k_diag<Cls_{g.tag}, 1>;")
             reg.append(f"    k->dg_threads = ND_THREADS;\n    k->dg_ppb = ND_THREADS;")
         info.update(roles=1, role_sizes=[g.nout], role_outs=[roles[0]], acc_groups=[])
-    elif len(roles) <= MAX_ROLES2:
+    elif len(roles) <= prm["max_roles2"]:
         mode = "staged2"
         for r, outs in enumerate(roles):
             code, _ = g.emit_role(f"{g.name}_r{r}", outs)
@@ -635,7 +652,7 @@ __global__ void __launch_bounds__(ND_THREADS, 2) k_s2_{g.tag}_r{r}(StagedArgs a)
     if constexpr (F32) stage_boys<{g.L}>(sboys, a.boysf);
     else stage_boys<{g.L}>(sboys, a.boys);
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= a.n) return;
+    if (t >= staged_count(a)) return;
     const uint2 q = staged_quartet(a, t);
     const GPair bra = a.bra[q.x];
     const GPair ket = a.ket[q.y];
@@ -656,7 +673,7 @@ __global__ void __launch_bounds__(ND_THREADS, 2) k_s2_{g.tag}_r{r}(StagedArgs a)
         info.update(roles=len(roles), role_sizes=[len(x) for x in roles], role_outs=roles, acc_groups=[])
     else:
         mode = "staged3"
-        groups = acc_groups(g)
+        groups = acc_groups(g, prm["acc_group"])
         keyidx = {}
         for gr in groups:
             for key in gr:
@@ -674,7 +691,7 @@ __global__ void __launch_bounds__(ND_THREADS, 2) k_sa_{g.tag}_r{r}(StagedArgs a)
     if constexpr (F32) stage_boys<{g.L}>(sboys, a.boysf);
     else stage_boys<{g.L}>(sboys, a.boys);
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= a.n) return;
+    if (t >= staged_count(a)) return;
     const uint2 q = staged_quartet(a, t);
     const GPair bra = a.bra[q.x];
     const GPair ket = a.ket[q.y];
@@ -682,14 +699,15 @@ __global__ void __launch_bounds__(ND_THREADS, 2) k_sa_{g.tag}_r{r}(StagedArgs a)
     else acc_{g.tag}_r{r}(bra, ket, a.prims, sboys, a.acc + (size_t){base} * a.stride + t, a.stride);
 }}""")
             base += len(gr)
-        outroles = [list(range(i, min(i + OUT_GROUP3, g.nout))) for i in range(0, g.nout, OUT_GROUP3)]
+        og = prm["out_group3"]
+        outroles = [list(range(i, min(i + og, g.nout))) for i in range(0, g.nout, og)]
         for r, outs in enumerate(outroles):
             code, _ = g.emit_hrr_role(f"hrr_{g.tag}_r{r}", outs, keyidx)
             funcs.append(code)
             kern.append(f"""
 __global__ void __launch_bounds__(ND_THREADS) k_sb_{g.tag}_r{r}(StagedArgs a) {{
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= a.n) return;
+    if (t >= staged_count(a)) return;
     const uint2 q = staged_quartet(a, t);
     const GPair bra = a.bra[q.x];
     const GPair ket = a.ket[q.y];

@@ -56,6 +56,14 @@ namespace {
 
 thread_local std::string g_err;
 
+// CUDA forbids device-synchronising calls (cudaMalloc/cudaFree/
+// cudaDeviceSynchronize/synchronous copies) in one thread while another
+// thread records a stream capture.  Handles live in different threads when
+// jobs are served concurrently, so captures and every such call of this
+// library take this lock.
+std::recursive_mutex g_dev_mu;
+#define HF_DEVICE_LOCK std::lock_guard<std::recursive_mutex> dev_lock_(g_dev_mu)
+
 #define HF_CHECK(call)                                                                   \
     do {                                                                                 \
         cudaError_t e_ = (call);                                                         \
@@ -194,6 +202,37 @@ __global__ void k_screen(ScreenArgs a) {
     }
 }
 
+// Sub-class ranges and list regions of the classes (fixed after the Schwarz
+// pass), passed by value to k_offsets.
+struct OffsetArgs {
+    int csub[NCLS + 1];      // sub-classes of class c: [csub[c], csub[c+1])
+    long long coff[NCLS];    // first entry of class c in the quartet buffer
+};
+
+// Write offsets of the compacted lists from the pass-0 counts, on the device
+// so that a build needs no host round trip: per class its FP64 entries, then
+// its FP32 entries, sub-classes in order.  Also stores the per-class totals
+// that the class kernels read.  One thread per class.
+__global__ void k_offsets(OffsetArgs o, ScreenSub* __restrict__ subs, const unsigned long long* __restrict__ cnt,
+                          unsigned long long* __restrict__ ncls) {
+    const int c = threadIdx.x;
+    if (c >= NCLS) return;
+    unsigned long long n64 = 0, n32 = 0;
+    for (int k = o.csub[c]; k < o.csub[c + 1]; ++k) {
+        n64 += cnt[2 * k];
+        n32 += cnt[2 * k + 1];
+    }
+    long long p64 = o.coff[c], p32 = o.coff[c] + (long long)n64;
+    for (int k = o.csub[c]; k < o.csub[c + 1]; ++k) {
+        subs[k].off[0] = p64;
+        subs[k].off[1] = p32;
+        p64 += (long long)cnt[2 * k];
+        p32 += (long long)cnt[2 * k + 1];
+    }
+    ncls[2 * c] = n64;
+    ncls[2 * c + 1] = n32;
+}
+
 // FMA-chain throughput probe: 8 independent chains per thread so the FP64 and
 // FP32 pipes, not latency, bound it.  Used to state the FP64/FP32 roofline.
 template <typename T>
@@ -275,13 +314,28 @@ struct hfgpu_handle {
     unsigned long long* d_cnt = nullptr;
     ClassStats* d_stats = nullptr;
     // last build statistics
-    long long st_pass[NCLS] = {}, st_scat[NCLS] = {}, st_prim[NCLS] = {}, st_f32[NCLS] = {};
     double st_ms[NCLS] = {};
     long long ntot = 0;
     long long ccap[NCLS] = {};      // candidates per class (upper bound of its list)
     long long coff[NCLS] = {};      // class region in the quartet buffer
     long long n64[NCLS] = {}, n32[NCLS] = {};
     cudaEvent_t ev[2 * NCLS + 2] = {};
+    int nsm = 148;
+    long long launches = 0;             // kernels enqueued by this handle (graph replays included)
+    long long graph_launches = 0;       // kernels in the captured build
+    OffsetArgs offs{};                  // sub-class ranges / list regions per class
+    unsigned long long* d_ncls = nullptr;  // [2 * NCLS] surviving quartets (FP64, FP32) per class
+    cudaGraph_t graph = nullptr;        // captured full build (hfgpu_graph_capture)
+    cudaGraphExec_t gexec = nullptr;
+    const void* gkey_f = nullptr;       // what the capture was recorded with
+    const void* gkey_p = nullptr;
+    double gkey_thr[3] = {};
+};
+
+struct hfgpu_batch {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<hfgpu_handle*> hs;  // launch accounting
 };
 
 namespace {
@@ -353,6 +407,7 @@ int download_f(hfgpu_handle* h, double* f) {
 int launch_maxdm(hfgpu_handle* h, const double* P, double* md = nullptr) {
     long long np = (long long)h->nsh * (h->nsh + 1) / 2;
     int blocks = (int)((np + 255) / 256);
+    ++h->launches;
     k_maxdm<<<blocks, 256, 0, h->stream>>>(h->d_shtyp, h->d_aosh, h->nsh, h->nb, P, md ? md : h->d_md);
     HF_CHECK(cudaGetLastError());
     return HFGPU_OK;
@@ -360,6 +415,7 @@ int launch_maxdm(hfgpu_handle* h, const double* P, double* md = nullptr) {
 
 int launch_symm(hfgpu_handle* h, double* F, const double* G = nullptr) {
     long long n = (long long)h->nb * h->nb;
+    ++h->launches;
     k_symm<<<(int)((n + 255) / 256), 256, 0, h->stream>>>(F, G ? G : h->d_G, h->nb);
     HF_CHECK(cudaGetLastError());
     return HFGPU_OK;
@@ -377,8 +433,7 @@ int run_staged_diag(hfgpu_handle* h, int t, int mode, const double* P, double th
         a.quartets = h->d_diaglist[t];
         a.n = m;
         a.q0 = q0;
-        a.from_back = 0;
-        a.cap = n;
+        a.ncls = nullptr;
         a.bra = h->d_pairs[t];
         a.ket = h->d_pairs[t];
         a.prims = h->psoa;
@@ -399,13 +454,16 @@ int run_staged_diag(hfgpu_handle* h, int t, int mode, const double* P, double th
         a.nsh = h->nsh;
         const int blocks = (m + ND_THREADS - 1) / ND_THREADS;
         for (int r = 0; r < K.nrole_a; ++r) {
+            ++h->launches;
             K.sa64[r]<<<blocks, ND_THREADS, 0, h->stream>>>(a);
             HF_CHECK(cudaGetLastError());
         }
         for (int r = 0; r < K.nrole_b; ++r) {
+            ++h->launches;
             K.sb64[r]<<<blocks, ND_THREADS, 0, h->stream>>>(a);
             HF_CHECK(cudaGetLastError());
         }
+        ++h->launches;
         (mode ? K.dscat1 : K.dscat0)<<<blocks, ND_THREADS, 0, h->stream>>>(a);
         HF_CHECK(cudaGetLastError());
     }
@@ -425,6 +483,7 @@ int launch_diag(hfgpu_handle* h, int mode, const double* P, double thr, double* 
         DiagArgs a{h->d_pairs[t], n, h->psoa, h->d_boys, h->d_schw[t], md ? md : h->d_md, h->nsh, P,
                    G ? G : h->d_G, h->nb, thr};
         const ClassKernels& K = CLASS_KERNELS[class_index(t, t)];
+        ++h->launches;
         diag_kernel(t, mode)<<<(n + K.dg_ppb - 1) / K.dg_ppb, K.dg_threads, 0, h->stream>>>(a);
         HF_CHECK(cudaGetLastError());
     }
@@ -444,6 +503,7 @@ size_t scratch_budget_doubles() {
 
 // Schwarz ordering (index_sort + find_threshold) and the active pair arrays.
 int build_active(hfgpu_handle* h) {
+    HF_DEVICE_LOCK;
     for (int t = 0; t < NPT; ++t) {
         int n = (int)h->pairs[t].size();
         h->schw[t].resize(n);
@@ -570,8 +630,11 @@ int build_active(hfgpu_handle* h) {
             }
         h->ccap[c] = ccap;
         h->coff[c] = qoff;
+        h->offs.coff[c] = qoff;
         qoff += ccap;
+        h->offs.csub[c + 1] = (int)h->hsubs.size();
     }
+    h->offs.csub[0] = 0;
     h->ntot = start;
     total_q = qoff;
     if (h->hsubs.size() > h->subcap) {
@@ -585,6 +648,12 @@ int build_active(hfgpu_handle* h) {
         rc = dalloc(&h->d_cnt, 2 * h->hsubs.size());
         if (rc) return rc;
         h->subcap = h->hsubs.size();
+    }
+    // the sub-class table stays on the device; k_offsets fills its offsets
+    if (!h->hsubs.empty()) {
+        HF_CHECK(cudaMemcpyAsync(h->d_subs, h->hsubs.data(), h->hsubs.size() * sizeof(ScreenSub),
+                                 cudaMemcpyHostToDevice, h->stream));
+        HF_CHECK(cudaStreamSynchronize(h->stream));
     }
     if ((size_t)total_q > h->qcap) {
         if (h->d_q) cudaFree(h->d_q);
@@ -630,12 +699,13 @@ int run_staged(hfgpu_handle* h, int c, int prec, long long n, const double* P, d
     const size_t st = h->stride[c];
     for (long long q0 = 0; q0 < n; q0 += (long long)st) {
         const int m = (int)std::min<long long>((long long)st, n - q0);
-        StagedArgs a;
-        a.quartets = h->d_q + h->coff[c] + (prec ? h->n64[c] : 0);
-        a.n = m;
+        StagedArgs a{};
+        a.quartets = h->d_q + h->coff[c];
+        a.n = m;  // the kernels clamp it by the device-side count
         a.q0 = q0;
-        a.from_back = 0;
-        a.cap = n;
+        a.ncls = h->d_ncls;
+        a.cls = c;
+        a.prec = prec;
         a.bra = h->d_apairs[K.bi];
         a.ket = h->d_apairs[K.ki];
         a.prims = h->apsoa;
@@ -655,28 +725,35 @@ int run_staged(hfgpu_handle* h, int c, int prec, long long n, const double* P, d
         a.stats = h->d_stats + c;
         const int blocks = (m + ND_THREADS - 1) / ND_THREADS;
         for (int r = 0; r < K.nrole_a; ++r) {
+            ++h->launches;
             (prec ? K.sa32[r] : K.sa64[r])<<<blocks, ND_THREADS, 0, stream>>>(a);
             HF_CHECK(cudaGetLastError());
         }
         for (int r = 0; r < K.nrole_b; ++r) {
+            ++h->launches;
             (prec ? K.sb32[r] : K.sb64[r])<<<blocks, ND_THREADS, 0, stream>>>(a);
             HF_CHECK(cudaGetLastError());
         }
+        ++h->launches;
         K.scat<<<blocks, ND_THREADS, 0, stream>>>(a);
         HF_CHECK(cudaGetLastError());
     }
     return HFGPU_OK;
 }
 
-int run_non_diag(hfgpu_handle* h, const double* P, double thr, int jonly, double f32cut) {
+// Off-diagonal build: the two screening passes with device-side offsets,
+// then the class kernels on NSTREAM concurrent streams.  With capture set,
+// nothing is read back on the host: every launch is sized by the class's
+// candidate count (an upper bound) and the kernels read the surviving count
+// from d_ncls, so the whole sequence can be recorded into a CUDA graph.
+// Eager builds read the counts back once to size the launches exactly.
+int run_non_diag(hfgpu_handle* h, const double* P, double thr, int jonly, double f32cut, bool capture = false) {
     if (!h->have_schwarz) return set_err(HFGPU_ERR_STATE, "fock_build_initial_diag has not been called");
     HF_CHECK(cudaMemsetAsync(h->d_stats, 0, NCLS * sizeof(ClassStats), h->stream));
+    HF_CHECK(cudaMemsetAsync(h->d_ncls, 0, 2 * NCLS * sizeof(unsigned long long), h->stream));
     const int nsub = (int)h->hsubs.size();
     for (int c = 0; c < NCLS; ++c) h->n64[c] = h->n32[c] = 0;
     if (h->ntot > 0 && nsub > 0) {
-        int dev = 0, nsm = 148;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         ScreenArgs sa{};
         sa.subs = h->d_subs;
         sa.nsub = nsub;
@@ -693,47 +770,28 @@ int run_non_diag(hfgpu_handle* h, const double* P, double thr, int jonly, double
         sa.cnt = h->d_cnt;
         sa.qbuf = h->d_q;
         const long long warps = h->ntot / 32;
-        const int blocks = (int)std::min<long long>((warps + 7) / 8, (long long)nsm * 64);
-        // pass 0: survivors per sub-class
-        HF_CHECK(cudaMemsetAsync(h->d_cnt, 0, 2 * nsub * sizeof(unsigned long long), h->stream));
-        HF_CHECK(cudaMemcpyAsync(h->d_subs, h->hsubs.data(), nsub * sizeof(ScreenSub), cudaMemcpyHostToDevice,
-                                 h->stream));
-        k_screen<0><<<blocks, 256, 0, h->stream>>>(sa);
+        const int blocks = (int)std::min<long long>((warps + 7) / 8, (long long)h->nsm * 64);
+        const size_t cbytes = 2 * (size_t)nsub * sizeof(unsigned long long);
+        HF_CHECK(cudaMemsetAsync(h->d_cnt, 0, cbytes, h->stream));
+        ++h->launches;
+        k_screen<0><<<blocks, 256, 0, h->stream>>>(sa);  // survivors per sub-class
         HF_CHECK(cudaGetLastError());
-        std::vector<unsigned long long> cnt(2 * nsub);
-        HF_CHECK(cudaMemcpyAsync(cnt.data(), h->d_cnt, cnt.size() * sizeof(unsigned long long),
-                                 cudaMemcpyDeviceToHost, h->stream));
-        HF_CHECK(cudaStreamSynchronize(h->stream));
-        // offsets: per class, FP64 entries then FP32 entries, sub-classes in order
-        for (int k = 0; k < nsub; ++k) {
-            const int c = h->hsubs[k].cls;
-            h->n64[c] += (long long)cnt[2 * k];
-            h->n32[c] += (long long)cnt[2 * k + 1];
-        }
-        long long p64[NCLS], p32[NCLS];
-        for (int c = 0; c < NCLS; ++c) {
-            p64[c] = h->coff[c];
-            p32[c] = h->coff[c] + h->n64[c];
-        }
-        for (int k = 0; k < nsub; ++k) {
-            const int c = h->hsubs[k].cls;
-            h->hsubs[k].off[0] = p64[c];
-            h->hsubs[k].off[1] = p32[c];
-            p64[c] += (long long)cnt[2 * k];
-            p32[c] += (long long)cnt[2 * k + 1];
-        }
-        // pass 1: compacted write
-        HF_CHECK(cudaMemsetAsync(h->d_cnt, 0, 2 * nsub * sizeof(unsigned long long), h->stream));
-        HF_CHECK(cudaMemcpyAsync(h->d_subs, h->hsubs.data(), nsub * sizeof(ScreenSub), cudaMemcpyHostToDevice,
-                                 h->stream));
-        k_screen<1><<<blocks, 256, 0, h->stream>>>(sa);
+        ++h->launches;
+        k_offsets<<<1, 32, 0, h->stream>>>(h->offs, h->d_subs, h->d_cnt, h->d_ncls);
         HF_CHECK(cudaGetLastError());
-        HF_CHECK(cudaStreamSynchronize(h->stream));  // hsubs is re-used as the copy source
+        HF_CHECK(cudaMemsetAsync(h->d_cnt, 0, cbytes, h->stream));
+        ++h->launches;
+        k_screen<1><<<blocks, 256, 0, h->stream>>>(sa);  // compacted write
+        HF_CHECK(cudaGetLastError());
     }
-    unsigned long long cnt[2 * NCLS];
-    for (int c = 0; c < NCLS; ++c) {
-        cnt[2 * c] = (unsigned long long)h->n64[c];
-        cnt[2 * c + 1] = (unsigned long long)h->n32[c];
+    if (!capture) {
+        unsigned long long cnt[2 * NCLS];
+        HF_CHECK(cudaMemcpyAsync(cnt, h->d_ncls, sizeof(cnt), cudaMemcpyDeviceToHost, h->stream));
+        HF_CHECK(cudaStreamSynchronize(h->stream));
+        for (int c = 0; c < NCLS; ++c) {
+            h->n64[c] = (long long)cnt[2 * c];
+            h->n32[c] = (long long)cnt[2 * c + 1];
+        }
     }
     // work items (class, precision) over NSTREAM concurrent streams, largest
     // first onto the least-loaded stream; with timing on, everything runs in
@@ -741,14 +799,14 @@ int run_non_diag(hfgpu_handle* h, const double* P, double thr, int jonly, double
     struct Item { int c, prec; long long n; double w; };
     std::vector<Item> items;
     for (int c = 0; c < NCLS; ++c) {
-        h->st_pass[c] = (long long)(cnt[2 * c] + cnt[2 * c + 1]);
         h->st_ms[c] = 0.0;
         for (int prec = 0; prec < 2; ++prec) {
-            const long long n = (long long)cnt[2 * c + prec];
+            long long n = prec ? h->n32[c] : h->n64[c];
+            if (capture) n = (prec && !(f32cut > 0.0)) ? 0 : h->ccap[c];
             if (n > 0) items.push_back({c, prec, n, (double)n * CLASS_KERNELS[c].nout});
         }
     }
-    const bool multi = !h->timing;
+    const bool multi = capture || !h->timing;
     if (multi) {
         std::stable_sort(items.begin(), items.end(), [](const Item& x, const Item& y) { return x.w > y.w; });
         HF_CHECK(cudaEventRecord(h->fork, h->stream));
@@ -765,19 +823,36 @@ int run_non_diag(hfgpu_handle* h, const double* P, double thr, int jonly, double
         load[k] += it.w;
         cudaStream_t st = multi ? h->aux[k] : h->stream;
         double* slot = h->d_scratch ? h->d_scratch + (multi ? (size_t)k * h->slot_doubles : 0) : nullptr;
-        if (h->timing) HF_CHECK(cudaEventRecord(h->ev[2 * c], h->stream));
+        const bool timed = h->timing && !multi;
+        if (timed) HF_CHECK(cudaEventRecord(h->ev[2 * c], h->stream));
         if (K.mode == 0) {
-            NDArgs a{h->d_q + h->coff[c] + (prec ? h->n64[c] : 0), (int)n, 0, n, h->d_apairs[K.bi],
-                     h->d_apairs[K.ki], h->apsoa, h->d_boys, h->d_boysf, P, h->d_G, h->nb, thr, jonly,
-                     h->d_stats + c};
+            NDArgs a{};
+            a.quartets = h->d_q + h->coff[c];
+            a.n = (int)n;
+            a.ncls = h->d_ncls;
+            a.cls = c;
+            a.prec = prec;
+            a.bra = h->d_apairs[K.bi];
+            a.ket = h->d_apairs[K.ki];
+            a.prims = h->apsoa;
+            a.boys = h->d_boys;
+            a.boysf = h->d_boysf;
+            a.P = P;
+            a.G = h->d_G;
+            a.nb = h->nb;
+            a.thr = thr;
+            a.jonly = jonly;
+            a.stats = h->d_stats + c;
             long long blocks = (n + K.nd_qpb - 1) / K.nd_qpb;
+            if (capture) blocks = std::min<long long>(blocks, (long long)h->nsm * 16);  // grid-stride
+            ++h->launches;
             (prec ? K.nd32 : K.nd64)<<<(int)blocks, K.nd_threads, 0, st>>>(a);
             HF_CHECK(cudaGetLastError());
         } else {
             int rc = run_staged(h, c, prec, n, P, thr, jonly, st, slot);
             if (rc) return rc;
         }
-        if (h->timing) {
+        if (timed) {
             HF_CHECK(cudaEventRecord(h->ev[2 * c + 1], h->stream));
             HF_CHECK(cudaEventSynchronize(h->ev[2 * c + 1]));
             float ms = 0;
@@ -791,14 +866,6 @@ int run_non_diag(hfgpu_handle* h, const double* P, double thr, int jonly, double
             HF_CHECK(cudaStreamWaitEvent(h->stream, h->join[k], 0));
         }
     }
-    ClassStats st[NCLS];
-    HF_CHECK(cudaMemcpyAsync(st, h->d_stats, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
-    HF_CHECK(cudaStreamSynchronize(h->stream));
-    for (int c = 0; c < NCLS; ++c) {
-        h->st_scat[c] = (long long)st[c].scattered;
-        h->st_prim[c] = (long long)st[c].prim;
-        h->st_f32[c] = (long long)st[c].fp32;
-    }
     return HFGPU_OK;
 }
 
@@ -809,6 +876,7 @@ extern "C" {
 const char* hfgpu_last_error(void) { return g_err.c_str(); }
 
 int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
+    HF_DEVICE_LOCK;
     if (!B || !out || B->nsh <= 0 || B->nb <= 0 || B->maxprim <= 0)
         return set_err(HFGPU_ERR_ARG, "hfgpu_init: bad arguments");
     *out = nullptr;
@@ -843,6 +911,11 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
         delete h;
         return set_err(HFGPU_ERR_CUDA, m);
     }
+    {
+        int dev = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (h->nsm <= 0) h->nsm = 148;
+    }
     int rc = 0;
     const size_t nb2 = (size_t)h->nb * h->nb;
     rc |= dalloc(&h->d_shtyp, h->nsh);
@@ -856,6 +929,7 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
     rc |= dalloc(&h->d_md, (size_t)h->nsh * h->nsh);
     rc |= dalloc(&h->d_cnt, 2 * NCLS);
     rc |= dalloc(&h->d_stats, NCLS);
+    rc |= dalloc(&h->d_ncls, 2 * NCLS);
     for (int t = 0; t < NPT; ++t) {
         size_t n = h->pairs[t].size();
         rc |= dalloc(&h->d_pairs[t], n);
@@ -923,6 +997,8 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
             return HFGPU_ERR_NOMEM;
         }
     }
+    if (ce == cudaSuccess) ce = cudaMemset(h->d_stats, 0, NCLS * sizeof(ClassStats));
+    if (ce == cudaSuccess) ce = cudaMemset(h->d_ncls, 0, 2 * NCLS * sizeof(unsigned long long));
     if (ce == cudaSuccess) ce = cudaDeviceSynchronize();
     if (ce != cudaSuccess) {
         std::string m = std::string("hfgpu_init: ") + cudaGetErrorString(ce);
@@ -935,9 +1011,13 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
 
 int hfgpu_finalize(hfgpu_handle* h) {
     if (!h) return HFGPU_OK;
+    HF_DEVICE_LOCK;
     if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    if (h->graph) cudaGraphDestroy(h->graph);
     void* bufs[] = {h->d_shtyp, h->d_aosh, h->d_psoa, h->d_apsoa, h->d_boys, h->d_boysf, h->d_P, h->d_F, h->d_G,
-                    h->d_md, h->d_subs, h->d_q, h->d_cnt, h->d_stats, h->d_scratch, h->d_dscratch};
+                    h->d_md, h->d_subs, h->d_q, h->d_cnt, h->d_stats, h->d_scratch, h->d_dscratch,
+                    h->d_ncls};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (int t = 0; t < NPT; ++t) {
@@ -960,8 +1040,19 @@ int hfgpu_finalize(hfgpu_handle* h) {
     return HFGPU_OK;
 }
 
+static void drop_graph(hfgpu_handle* h) {
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    h->gexec = nullptr;
+    h->graph = nullptr;
+}
+
 int hfgpu_fock_build_initial_diag(hfgpu_handle* h, double* f, const double* p, double thr) {
     if (!h || !f || !p) return set_err(HFGPU_ERR_ARG, "null argument");
+    {
+        HF_DEVICE_LOCK;
+        drop_graph(h);  // the Schwarz pass re-sizes the buffers a captured build points at
+    }
     int rc = upload_fp(h, f, p);
     if (rc) return rc;
     HF_CHECK(cudaMemsetAsync(h->d_G, 0, (size_t)h->nb * h->nb * sizeof(double), h->stream));
@@ -1010,16 +1101,131 @@ int hfgpu_fock_build_non_diag_mixed(hfgpu_handle* h, double* f, const double* p,
     return non_diag_host(h, f, p, thr, 0, fp32_cutoff);
 }
 
-int hfgpu_fock_build_device(hfgpu_handle* h, double* f_dev, const double* p_dev, double thr_diag,
-                            double thr_non_diag, double fp32_cutoff) {
-    if (!h || !f_dev || !p_dev) return set_err(HFGPU_ERR_ARG, "null argument");
-    if (!h->have_schwarz) return set_err(HFGPU_ERR_STATE, "fock_build_initial_diag has not been called");
+static int device_build(hfgpu_handle* h, double* f_dev, const double* p_dev, double thr_diag, double thr_non_diag,
+                        double fp32_cutoff, bool capture) {
     int rc;
     HF_CHECK(cudaMemsetAsync(h->d_G, 0, (size_t)h->nb * h->nb * sizeof(double), h->stream));
     if ((rc = launch_maxdm(h, p_dev))) return rc;
     if ((rc = launch_diag(h, 1, p_dev, thr_diag))) return rc;
-    if ((rc = run_non_diag(h, p_dev, thr_non_diag, 0, fp32_cutoff))) return rc;
+    if ((rc = run_non_diag(h, p_dev, thr_non_diag, 0, fp32_cutoff, capture))) return rc;
     return launch_symm(h, f_dev);
+}
+
+int hfgpu_fock_build_device(hfgpu_handle* h, double* f_dev, const double* p_dev, double thr_diag,
+                            double thr_non_diag, double fp32_cutoff) {
+    if (!h || !f_dev || !p_dev) return set_err(HFGPU_ERR_ARG, "null argument");
+    if (!h->have_schwarz) return set_err(HFGPU_ERR_STATE, "fock_build_initial_diag has not been called");
+    return device_build(h, f_dev, p_dev, thr_diag, thr_non_diag, fp32_cutoff, false);
+}
+
+int hfgpu_graph_capture(hfgpu_handle* h, double* f_dev, const double* p_dev, double thr_diag, double thr_non_diag,
+                        double fp32_cutoff) {
+    if (!h || !f_dev || !p_dev) return set_err(HFGPU_ERR_ARG, "null argument");
+    if (!h->have_schwarz) return set_err(HFGPU_ERR_STATE, "fock_build_initial_diag has not been called");
+    HF_CHECK(cudaStreamSynchronize(h->stream));
+    HF_DEVICE_LOCK;  // held from the start of the capture to its end
+    drop_graph(h);
+    const long long before = h->launches;
+    // thread-local mode: other host threads (other jobs, the caller's own
+    // framework) may keep allocating while this thread records
+    HF_CHECK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = device_build(h, f_dev, p_dev, thr_diag, thr_non_diag, fp32_cutoff, true);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(h->stream, &g);  // always ends the capture
+    if (rc != HFGPU_OK || ce != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        if (rc != HFGPU_OK) return rc;
+        return set_err(HFGPU_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ce));
+    }
+    h->graph = g;
+    h->graph_launches = h->launches - before;
+    h->launches = before;  // recorded, not run
+    h->gkey_f = f_dev;
+    h->gkey_p = p_dev;
+    h->gkey_thr[0] = thr_diag;
+    h->gkey_thr[1] = thr_non_diag;
+    h->gkey_thr[2] = fp32_cutoff;
+    const cudaError_t ie = cudaGraphInstantiate(&h->gexec, g, 0);
+    if (ie != cudaSuccess) {
+        h->gexec = nullptr;
+        drop_graph(h);
+        return set_err(HFGPU_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ie));
+    }
+    return HFGPU_OK;
+}
+
+int hfgpu_graph_launch(hfgpu_handle* h) {
+    if (!h) return set_err(HFGPU_ERR_ARG, "null handle");
+    if (!h->gexec) return set_err(HFGPU_ERR_STATE, "hfgpu_graph_capture has not been called");
+    HF_CHECK(cudaGraphLaunch(h->gexec, h->stream));
+    h->launches += h->graph_launches;
+    return HFGPU_OK;
+}
+
+int hfgpu_fock_build_graph(hfgpu_handle* h, double* f, const double* p, double thr_diag, double thr_non_diag,
+                           double fp32_cutoff) {
+    if (!h || !f || !p) return set_err(HFGPU_ERR_ARG, "null argument");
+    if (!h->have_schwarz) return set_err(HFGPU_ERR_STATE, "fock_build_initial_diag has not been called");
+    const bool same = h->gexec && h->gkey_f == h->d_F && h->gkey_p == h->d_P && h->gkey_thr[0] == thr_diag &&
+                      h->gkey_thr[1] == thr_non_diag && h->gkey_thr[2] == fp32_cutoff;
+    int rc;
+    if (!same && (rc = hfgpu_graph_capture(h, h->d_F, h->d_P, thr_diag, thr_non_diag, fp32_cutoff))) return rc;
+    if ((rc = upload_fp(h, f, p))) return rc;
+    HF_CHECK(cudaGraphLaunch(h->gexec, h->stream));
+    h->launches += h->graph_launches;
+    return download_f(h, f);
+}
+
+int hfgpu_synchronize(hfgpu_handle* h) {
+    if (!h) return set_err(HFGPU_ERR_ARG, "null handle");
+    HF_CHECK(cudaStreamSynchronize(h->stream));
+    return HFGPU_OK;
+}
+
+int hfgpu_batch_create(hfgpu_handle* const* hs, int n, hfgpu_batch** out) {
+    if (!hs || !out || n <= 0) return set_err(HFGPU_ERR_ARG, "hfgpu_batch_create: bad arguments");
+    *out = nullptr;
+    for (int i = 0; i < n; ++i) {
+        if (!hs[i]) return set_err(HFGPU_ERR_ARG, "hfgpu_batch_create: null handle");
+        if (!hs[i]->graph)
+            return set_err(HFGPU_ERR_STATE, "hfgpu_batch_create: handle " + std::to_string(i) +
+                                                " has no captured build (call hfgpu_graph_capture)");
+        for (int j = 0; j < i; ++j)
+            if (hs[j] == hs[i]) return set_err(HFGPU_ERR_ARG, "hfgpu_batch_create: a handle appears twice");
+    }
+    HF_DEVICE_LOCK;
+    hfgpu_batch* b = new hfgpu_batch();
+    b->hs.assign(hs, hs + n);
+    cudaError_t ce = cudaGraphCreate(&b->graph, 0);
+    // one child graph per instance, no edges between them: the instances
+    // share nothing on the device and run concurrently
+    for (int i = 0; i < n && ce == cudaSuccess; ++i) {
+        cudaGraphNode_t node;
+        ce = cudaGraphAddChildGraphNode(&node, b->graph, nullptr, 0, hs[i]->graph);
+    }
+    if (ce == cudaSuccess) ce = cudaGraphInstantiate(&b->exec, b->graph, 0);
+    if (ce != cudaSuccess) {
+        hfgpu_batch_destroy(b);
+        return set_err(HFGPU_ERR_CUDA, std::string("hfgpu_batch_create: ") + cudaGetErrorString(ce));
+    }
+    *out = b;
+    return HFGPU_OK;
+}
+
+int hfgpu_batch_launch(hfgpu_batch* b, void* stream) {
+    if (!b || !b->exec) return set_err(HFGPU_ERR_ARG, "null batch");
+    HF_CHECK(cudaGraphLaunch(b->exec, (cudaStream_t)stream));
+    for (hfgpu_handle* h : b->hs) h->launches += h->graph_launches;
+    return HFGPU_OK;
+}
+
+int hfgpu_batch_destroy(hfgpu_batch* b) {
+    if (!b) return HFGPU_OK;
+    HF_DEVICE_LOCK;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    delete b;
+    return HFGPU_OK;
 }
 
 int hfgpu_set_scratch_budget(hfgpu_handle* h, size_t bytes) {
@@ -1077,13 +1283,27 @@ int hfgpu_get_schwarz(const hfgpu_handle* h, double* schw_sh, int* last) {
 int hfgpu_get_class_stats(const hfgpu_handle* h, long long* n_pass, long long* n_scattered, long long* n_prim,
                           long long* n_fp32, double* ms) {
     if (!h) return set_err(HFGPU_ERR_ARG, "null handle");
+    // the counters live on the device (a captured build never returns to the
+    // host); read them after the handle's stream has drained
+    ClassStats st[NCLS];
+    unsigned long long cnt[2 * NCLS];
+    HF_DEVICE_LOCK;
+    HF_CHECK(cudaStreamSynchronize(h->stream));
+    HF_CHECK(cudaMemcpy(st, h->d_stats, sizeof(st), cudaMemcpyDeviceToHost));
+    HF_CHECK(cudaMemcpy(cnt, h->d_ncls, sizeof(cnt), cudaMemcpyDeviceToHost));
     for (int c = 0; c < NCLS; ++c) {
-        if (n_pass) n_pass[c] = h->st_pass[c];
-        if (n_scattered) n_scattered[c] = h->st_scat[c];
-        if (n_prim) n_prim[c] = h->st_prim[c];
-        if (n_fp32) n_fp32[c] = h->st_f32[c];
+        if (n_pass) n_pass[c] = (long long)(cnt[2 * c] + cnt[2 * c + 1]);
+        if (n_scattered) n_scattered[c] = (long long)st[c].scattered;
+        if (n_prim) n_prim[c] = (long long)st[c].prim;
+        if (n_fp32) n_fp32[c] = (long long)st[c].fp32;
         if (ms) ms[c] = h->st_ms[c];
     }
+    return HFGPU_OK;
+}
+
+int hfgpu_launch_count(const hfgpu_handle* h, long long* n) {
+    if (!h || !n) return set_err(HFGPU_ERR_ARG, "null argument");
+    *n = h->launches;
     return HFGPU_OK;
 }
 
@@ -1096,6 +1316,7 @@ int hfgpu_set_timing(hfgpu_handle* h, int on) {
 void* hfgpu_stream(hfgpu_handle* h) { return h ? (void*)h->stream : nullptr; }
 
 int hfgpu_measure_fma_peak(double* fp64_gflops, double* fp32_gflops) {
+    HF_DEVICE_LOCK;
     int dev = 0, nsm = 0;
     HF_CHECK(cudaGetDevice(&dev));
     HF_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));

@@ -62,6 +62,14 @@ def _load():
     lib.hfgpu_fock_build_diag_static.argtypes = [vp, vp, vp, ctypes.c_double]
     lib.hfgpu_set_scratch_budget.argtypes = [vp, ctypes.c_size_t]
     lib.hfgpu_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
+    lib.hfgpu_graph_capture.argtypes = [vp, vp, vp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+    lib.hfgpu_graph_launch.argtypes = [vp]
+    lib.hfgpu_synchronize.argtypes = [vp]
+    lib.hfgpu_launch_count.argtypes = [vp, ll]
+    lib.hfgpu_fock_build_graph.argtypes = [vp, d, d, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+    lib.hfgpu_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp)]
+    lib.hfgpu_batch_launch.argtypes = [vp, vp]
+    lib.hfgpu_batch_destroy.argtypes = [vp]
     return lib
 
 
@@ -73,7 +81,9 @@ EXPORTS = ["hfgpu_init", "hfgpu_fock_build_initial_diag", "hfgpu_fock_build_diag
            "hfgpu_get_schwarz", "hfgpu_get_class_stats", "hfgpu_set_timing", "hfgpu_stream",
            "hfgpu_finalize", "hfgpu_last_error", "hfgpu_measure_fma_peak",
            "hfgpu_fock_build_diag_static", "hfgpu_one_electron", "hfgpu_set_scratch_budget",
-           "hfgpu_device_bytes"]
+           "hfgpu_device_bytes", "hfgpu_graph_capture", "hfgpu_graph_launch", "hfgpu_synchronize",
+           "hfgpu_fock_build_graph", "hfgpu_launch_count",
+           "hfgpu_batch_create", "hfgpu_batch_launch", "hfgpu_batch_destroy"]
 
 
 def measure_fma_peak():
@@ -166,6 +176,28 @@ class FockBuilder:
         _check(_lib.hfgpu_fock_build_diag_static(self.h, ctypes.c_void_p(f_ptr), ctypes.c_void_p(p_ptr),
                                                  float(thr)), "fock_build_diag_static")
 
+    def graph_capture(self, f_ptr: int, p_ptr: int, thr_diag: float, thr_non_diag: float,
+                      fp32_cutoff: float = 0.0):
+        """Records fock_build_device on these device pointers as a CUDA graph
+        (replayed by graph_launch; nothing runs now)."""
+        _check(_lib.hfgpu_graph_capture(self.h, ctypes.c_void_p(f_ptr), ctypes.c_void_p(p_ptr), float(thr_diag),
+                                        float(thr_non_diag), float(fp32_cutoff)), "graph_capture")
+
+    def fock_build_graph(self, f: np.ndarray, p: np.ndarray, thr_diag: float, thr_non_diag: float,
+                         fp32_cutoff: float = 0.0):
+        """f += G(p): fock_build_diag(thr_diag) + fock_build_non_diag(thr_non_diag)
+        (mixed with fp32_cutoff > 0) as one CUDA-graph replay, host arrays."""
+        fp, pp, keep = self._fp(f, p)
+        _check(_lib.hfgpu_fock_build_graph(self.h, fp, pp, float(thr_diag), float(thr_non_diag),
+                                           float(fp32_cutoff)), "fock_build_graph")
+
+    def graph_launch(self):
+        """Enqueues one replay of the captured build on the handle's stream."""
+        _check(_lib.hfgpu_graph_launch(self.h), "graph_launch")
+
+    def synchronize(self):
+        _check(_lib.hfgpu_synchronize(self.h), "synchronize")
+
     def set_scratch_budget(self, nbytes: int):
         _check(_lib.hfgpu_set_scratch_budget(self.h, int(nbytes)), "set_scratch_budget")
 
@@ -173,6 +205,12 @@ class FockBuilder:
         b = ctypes.c_size_t()
         _check(_lib.hfgpu_device_bytes(self.h, ctypes.byref(b)), "device_bytes")
         return int(b.value)
+
+    def launch_count(self) -> int:
+        """Kernels enqueued by this handle so far (graph replays included)."""
+        n = ctypes.c_longlong()
+        _check(_lib.hfgpu_launch_count(self.h, ctypes.byref(n)), "launch_count")
+        return int(n.value)
 
     def stream(self) -> int:
         return int(_lib.hfgpu_stream(self.h) or 0)
@@ -194,3 +232,28 @@ class FockBuilder:
         out = {k: np.array(list(a), dtype=np.int64) for k, a in zip(keys, arrs)}
         out["ms"] = np.array(list(ms))
         return out
+
+
+class Batch:
+    """Captured builds of several FockBuilders replayed as one graph launch."""
+
+    def __init__(self, builders):
+        self.builders = list(builders)  # keeps the handles alive
+        arr = (ctypes.c_void_p * len(self.builders))(*[b.h.value for b in self.builders])
+        out = ctypes.c_void_p()
+        _check(_lib.hfgpu_batch_create(arr, len(self.builders), ctypes.byref(out)), "batch_create")
+        self.b = out
+
+    def launch(self, stream: int = 0):
+        _check(_lib.hfgpu_batch_launch(self.b, ctypes.c_void_p(stream)), "batch_launch")
+
+    def close(self):
+        if getattr(self, "b", None):
+            _lib.hfgpu_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -59,13 +59,17 @@ def direct_hartreefock(mol: Molecule, sh: ShellSet, builder, p_guess: Optional[n
                        maxiter: int = 25, conv: float = 1e-5, conve: float = 5e-8,
                        lowthresh: float = 5e-7, fdifffac: float = 0.1, ndiis: int = 8,
                        levshft: Optional[float] = None, ints=None, log: Optional[Callable] = None,
-                       fp32_cutoff: float = 0.0) -> SCFResult:
+                       fp32_cutoff: float = 0.0, graph: bool = False) -> SCFResult:
     """Runs the reference's direct SCF protocol with `builder`.
 
     fp32_cutoff > 0 selects the mixed-precision form for the incremental
     (delta-P) builds: quartets whose screening bound on dP falls below the
     cutoff are evaluated in FP32 by builder.fock_build_non_diag_mixed; full
-    builds, accumulation, DIIS, the eigensolve and the energy stay FP64."""
+    builds, accumulation, DIIS, the eigensolve and the energy stay FP64.
+
+    graph=True runs every build after the first as one CUDA-graph replay
+    (builder.fock_build_graph: diag + non-diag fused, with the same
+    thresholds and arithmetic as the two separate calls)."""
     nb = sh.nb
     nocc = mol.nocc
     S, T, V = ints if ints is not None else onee.one_electron(mol, sh)
@@ -114,19 +118,25 @@ def direct_hartreefock(mol: Molecule, sh: ShellSet, builder, p_guess: Optional[n
             nfull = 0
             kind = "initial"
         elif fullfock:
-            builder.fock_build_diag(f, p, thresh)
-            builder.fock_build_non_diag(f, p, thresh)
+            if graph:
+                builder.fock_build_graph(f, p, thresh, thresh, 0.0)
+            else:
+                builder.fock_build_diag(f, p, thresh)
+                builder.fock_build_non_diag(f, p, thresh)
             fullfock = False
             nfull = 0
             kind = "full"
         else:
             delp = p - pold
             delf = np.zeros((nb, nb))
-            builder.fock_build_diag(delf, delp, thresh)
-            if fp32_cutoff > 0.0:
-                builder.fock_build_non_diag_mixed(delf, delp, thresh * fdifffac, fp32_cutoff)
+            if graph:
+                builder.fock_build_graph(delf, delp, thresh, thresh * fdifffac, fp32_cutoff)
             else:
-                builder.fock_build_non_diag(delf, delp, thresh * fdifffac)
+                builder.fock_build_diag(delf, delp, thresh)
+                if fp32_cutoff > 0.0:
+                    builder.fock_build_non_diag_mixed(delf, delp, thresh * fdifffac, fp32_cutoff)
+                else:
+                    builder.fock_build_non_diag(delf, delp, thresh * fdifffac)
             f = faobold + delf
             nfull += 1
             if nfull == 15:

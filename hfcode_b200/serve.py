@@ -86,7 +86,8 @@ def estimate_footprint(sh: ShellSet, scratch_budget: int) -> int:
 
 class Server:
     def __init__(self, hbm_budget: int, max_slots: int = 8, scratch_budget: int = 256 << 20,
-                 fp32_cutoff: float = 1e-7, conve: float = 1e-8, conv: float = 1e-6, basis_name: str = "6-31G(d)"):
+                 fp32_cutoff: float = 1e-7, conve: float = 1e-8, conv: float = 1e-6, basis_name: str = "6-31G(d)",
+                 graphs: bool = True):
         from . import fock  # loads the CUDA library; fails loudly without it
         self.fock = fock
         self.hbm_budget = hbm_budget
@@ -94,6 +95,7 @@ class Server:
         self.scratch_budget = scratch_budget
         self.fp32_cutoff = fp32_cutoff
         self.conve, self.conv = conve, conv
+        self.graphs = graphs  # builds after the first as CUDA-graph replays
         self.basis = basismod.load_basis(basis_name)
         self.lock = threading.Condition()
         self.in_use = 0
@@ -149,7 +151,8 @@ class Server:
 
             ints = onee.one_electron(job.mol, job.sh)
             r = scf.direct_hartreefock(job.mol, job.sh, Tracked(fb), p_guess=job.p0, conve=self.conve,
-                                       conv=self.conv, maxiter=60, ints=ints, fp32_cutoff=self.fp32_cutoff)
+                                       conv=self.conv, maxiter=60, ints=ints, fp32_cutoff=self.fp32_cutoff,
+                                       graph=self.graphs)
             job.energy, job.cycles, job.converged = r.energy, r.cycles, r.converged
         except Exception as e:  # the job fails, the server keeps serving
             job.error = f"{type(e).__name__}: {e}"
@@ -194,6 +197,7 @@ class Server:
                 "service_ms": {"p50": float(np.percentile(svc, 50)), "p99": float(np.percentile(svc, 99))},
                 "queue_ms": {"p50": float(np.percentile(que, 50)), "p99": float(np.percentile(que, 99))},
                 "failed": sum(1 for j in jobs if j.error), "not_converged": sum(1 for j in jobs if not j.converged),
+                "errors": sorted({j.error for j in jobs if j.error})[:5],
                 "peak_active": self.peak_active, "peak_hbm_bytes": self.peak_in_use,
                 "max_slots": self.max_slots, "hbm_budget": self.hbm_budget, "fp32_cutoff": self.fp32_cutoff}
 
@@ -225,14 +229,17 @@ def main():
     ap.add_argument("--hbm-gb", type=float, default=64.0)
     ap.add_argument("--fp32-cutoff", type=float, default=1e-7)
     ap.add_argument("--sequential", action="store_true", help="also run the plain per-job form")
+    ap.add_argument("--no-graphs", action="store_true", help="separate diag / non-diag calls per build")
     args = ap.parse_args()
-    srv = Server(int(args.hbm_gb * (1 << 30)), args.slots, fp32_cutoff=args.fp32_cutoff)
+    srv = Server(int(args.hbm_gb * (1 << 30)), args.slots, fp32_cutoff=args.fp32_cutoff,
+                 graphs=not args.no_graphs)
     jobs = make_stream(args.jobs, args.rate)
     out = {"served": srv.serve(jobs)}
     if args.sequential:
         seq = make_stream(args.jobs, args.rate)
         out["sequential"] = serve_sequential(seq, Server(int(args.hbm_gb * (1 << 30)), 1,
-                                                        fp32_cutoff=args.fp32_cutoff))
+                                                        fp32_cutoff=args.fp32_cutoff,
+                                                        graphs=not args.no_graphs))
     print(json.dumps(out))
 
 

@@ -74,10 +74,47 @@ int hfgpu_fock_build_non_diag_mixed(hfgpu_handle* h, double* f, const double* p,
 /* Device-resident variant for callers that keep F and P in HBM: one full
  * build (fock_build_diag with thr_diag + fock_build_non_diag with
  * thr_non_diag, optionally mixed) on device pointers, enqueued on the
- * handle's stream without host synchronisation except for reading the
- * per-class quartet counts.  f_dev += G(p_dev). */
+ * handle's stream; the host waits once, to read the per-class quartet
+ * counts that size the launches.  f_dev += G(p_dev). */
 int hfgpu_fock_build_device(hfgpu_handle* h, double* f_dev, const double* p_dev, double thr_diag,
                             double thr_non_diag, double fp32_cutoff);
+
+/* Batching form: the whole device build above recorded once as a CUDA graph
+ * and replayed with one launch per build.  The 46 per-class loops of
+ * fock_build_non_diag.f90 (and the diagonal builders) become one graph of
+ * kernels on four concurrent branches; the per-class quartet counts stay on
+ * the device, so a replay never returns to the host.  No counterpart in the
+ * reference.
+ *
+ * hfgpu_graph_capture records f_dev += G(p_dev) with the given thresholds
+ * and cutoff (replacing any earlier capture); the pointers are baked in, so
+ * replays read whatever p_dev holds at that time.  It does not run the
+ * build.  hfgpu_fock_build_initial_diag drops the capture (it re-sizes the
+ * buffers the graph uses).  hfgpu_graph_launch enqueues one replay on the
+ * handle's stream and returns; hfgpu_synchronize waits for the stream. */
+int hfgpu_graph_capture(hfgpu_handle* h, double* f_dev, const double* p_dev, double thr_diag,
+                        double thr_non_diag, double fp32_cutoff);
+int hfgpu_graph_launch(hfgpu_handle* h);
+int hfgpu_synchronize(hfgpu_handle* h);
+
+/* The same replay behind the reference-style host interface: f += G(p) on
+ * host arrays (fock_build_diag with thr_diag + fock_build_non_diag with
+ * thr_non_diag, optionally mixed), through the handle's own device F and P
+ * and a capture kept per (thresholds, cutoff) -- re-recorded when they
+ * change.  One upload, one graph launch and one download per call. */
+int hfgpu_fock_build_graph(hfgpu_handle* h, double* f, const double* p, double thr_diag, double thr_non_diag,
+                           double fp32_cutoff);
+
+/* Several SCF instances' captured builds as one graph launch: one child
+ * graph per handle, no dependencies between them, so independent molecules
+ * fill the GPU together.  Every handle must hold a capture (and appear
+ * once); the batch copies the captures, stays valid while the handles live
+ * and are not re-initialised, and is launched on any stream (NULL = the
+ * legacy default stream). */
+typedef struct hfgpu_batch hfgpu_batch;
+int hfgpu_batch_create(hfgpu_handle* const* hs, int n, hfgpu_batch** out);
+int hfgpu_batch_launch(hfgpu_batch* b, void* stream);
+int hfgpu_batch_destroy(hfgpu_batch* b);
 
 /* Number of basis functions / shells / shell pairs of the handle. */
 int hfgpu_dims(const hfgpu_handle* h, int* nb, int* nsh, int* npairs);
@@ -95,6 +132,10 @@ int hfgpu_get_schwarz(const hfgpu_handle* h, double* schw_sh, int* last);
  * (mixed form), and the kernel time in ms (0 unless timing is enabled). */
 int hfgpu_get_class_stats(const hfgpu_handle* h, long long* n_pass, long long* n_scattered,
                           long long* n_prim, long long* n_fp32, double* ms);
+
+/* Kernels this handle has enqueued since hfgpu_init (graph and batch
+ * replays count their captured kernels). */
+int hfgpu_launch_count(const hfgpu_handle* h, long long* n);
 
 /* Enable (1) or disable (0) per-class CUDA-event timing of the off-diagonal
  * kernels. */

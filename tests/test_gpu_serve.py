@@ -14,7 +14,7 @@ def test_served_results_match_alone():
     jobs_mix = serve.make_stream(10, rate=0.0, seed=4242, max_alkane=5, max_water=4)
     srv = serve.Server(hbm_budget=32 << 30, max_slots=4, fp32_cutoff=1e-7)
     out = srv.serve(jobs_mix, realtime=False)
-    assert out["failed"] == 0 and out["not_converged"] == 0
+    assert out["failed"] == 0 and out["not_converged"] == 0, out["errors"]
     assert 1 <= srv.peak_active <= 4
     jobs_alone = serve.make_stream(10, rate=0.0, seed=4242, max_alkane=5, max_water=4)
     solo = serve.Server(hbm_budget=32 << 30, max_slots=1, fp32_cutoff=1e-7)
@@ -35,6 +35,6 @@ def test_admission_waits_for_memory():
     fps = sorted(j.footprint for j in jobs)
     srv = serve.Server(hbm_budget=fps[-1] + fps[-2], max_slots=8)
     out = srv.serve(jobs, realtime=False)
-    assert out["failed"] == 0
+    assert out["failed"] == 0, out["errors"]
     assert srv.peak_in_use <= fps[-1] + fps[-2]
     assert srv.peak_active <= 6
