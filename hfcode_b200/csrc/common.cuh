@@ -330,6 +330,138 @@ __device__ __forceinline__ uint2 staged_quartet(const StagedArgs& a, int t) {
     return a.quartets[i];
 }
 
+// ------------------------------------------- staged scatter, async loads ----
+// The staged scatter reads each quartet's ERI block (one column of the
+// scratch rows) once.  With ~255 registers per thread only 8 warps fit on an
+// SM, too few to hide the latency of plain loads, so the block's rows are
+// streamed into shared memory with per-thread cp.async copies: slab s (the
+// NC*ND rows of one (i, j)) is consumed while slabs s+1 .. s+NBUF-1 are in
+// flight.  Every thread copies and reads only its own column, so no block
+// barrier is needed; cp.async.wait_group bounds each wait by the thread's own
+// copies.  P_bc and P_bd, needed for every i, are staged once in shared
+// memory as well.
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Shared-memory plan of the async scatter: three slab buffers when they fit
+// two blocks per SM, else two.
+__host__ __device__ constexpr int scat_nbuf(int NA, int NB, int NC, int ND) {
+    return (3 * NC * ND + NB * (NC + ND)) * ND_THREADS * 8 <= 110 * 1024 ? 3 : 2;
+}
+__host__ __device__ constexpr int scat_smem_bytes(int NA, int NB, int NC, int ND) {
+    return (scat_nbuf(NA, NB, NC, ND) * NC * ND + NB * (NC + ND)) * ND_THREADS * 8;
+}
+
+template <int NA, int NB, int NC, int ND>
+__device__ __forceinline__ void scatter_async(const double* __restrict__ e, size_t st, double s, const GPair& bra,
+                                              const GPair& ket, const double* __restrict__ P,
+                                              double* __restrict__ G, int nb, bool jonly, double* sm) {
+    constexpr int T = ND_THREADS, SLAB = NC * ND, NS = NA * NB, NBUF = scat_nbuf(NA, NB, NC, ND);
+    const int tid = threadIdx.x;
+    const int a0 = bra.aoa, b0 = bra.aob, c0 = ket.aoa, d0 = ket.aob;
+    auto Pm = [&](int r, int c) { return __ldg(P + r + (size_t)c * nb); };
+    auto Ga = [&](int r, int c) { return G + r + (size_t)c * nb; };
+    double* eb = sm + tid;                      // [NBUF][SLAB][T], this thread's column
+    double* pk = sm + NBUF * SLAB * T + tid;    // [NB*NC] P_bc then [NB*ND] P_bd
+    auto issue = [&](int slab) {
+        if (slab < NS) {
+            const double* src = e + (size_t)slab * SLAB * st;
+            double* dst = eb + (slab % NBUF) * SLAB * T;
+#pragma unroll
+            for (int r = 0; r < SLAB; ++r) cp_async8(dst + r * T, src + (size_t)r * st);
+        }
+        cp_async_commit();  // empty groups keep the count uniform
+    };
+#pragma unroll
+    for (int q = 0; q < NBUF - 1; ++q) issue(q);
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+#pragma unroll
+        for (int k = 0; k < NC; ++k) pk[(j * NC + k) * T] = Pm(b0 + j, c0 + k);
+#pragma unroll
+        for (int l = 0; l < ND; ++l) pk[(NB * NC + j * ND + l) * T] = Pm(b0 + j, d0 + l);
+    }
+    const double s2 = 2.0 * s, hs = -0.5 * s;
+    double jcd[NC * ND], kbc[NB * NC], kbd[NB * ND], pcd[NC * ND];
+#pragma unroll
+    for (int x = 0; x < NC * ND; ++x) jcd[x] = 0.0;
+#pragma unroll
+    for (int x = 0; x < NB * NC; ++x) kbc[x] = 0.0;
+#pragma unroll
+    for (int x = 0; x < NB * ND; ++x) kbd[x] = 0.0;
+#pragma unroll
+    for (int k = 0; k < NC; ++k)
+#pragma unroll
+        for (int l = 0; l < ND; ++l) pcd[k * ND + l] = Pm(c0 + k, d0 + l);
+#pragma unroll 1
+    for (int i = 0; i < NA; ++i) {
+        double jab[NB], kac[NC], kad[ND], pad_[ND], pac[NC];
+#pragma unroll
+        for (int j = 0; j < NB; ++j) jab[j] = 0.0;
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+            kac[k] = 0.0;
+            pac[k] = Pm(a0 + i, c0 + k);
+        }
+#pragma unroll
+        for (int l = 0; l < ND; ++l) {
+            kad[l] = 0.0;
+            pad_[l] = Pm(a0 + i, d0 + l);
+        }
+#pragma unroll
+        for (int j = 0; j < NB; ++j) {
+            const int slab = i * NB + j;
+            issue(slab + NBUF - 1);
+            cp_async_wait<NBUF - 1>();  // this thread's copies of `slab` have landed
+            const double* es = eb + (slab % NBUF) * SLAB * T;
+            const double pab = Pm(a0 + i, b0 + j);
+#pragma unroll
+            for (int k = 0; k < NC; ++k) {
+                const double pbc = pk[(j * NC + k) * T];
+#pragma unroll
+                for (int l = 0; l < ND; ++l) {
+                    const double v = es[(k * ND + l) * T];
+                    jab[j] += pcd[k * ND + l] * v;
+                    jcd[k * ND + l] += pab * v;
+                    if (!jonly) {
+                        kac[k] += pk[(NB * NC + j * ND + l) * T] * v;
+                        kad[l] += pbc * v;
+                        kbc[j * NC + k] += pad_[l] * v;
+                        kbd[j * ND + l] += pac[k] * v;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < NB; ++j) atomicAdd(Ga(a0 + i, b0 + j), s2 * jab[j]);
+        if (!jonly) {
+#pragma unroll
+            for (int k = 0; k < NC; ++k) atomicAdd(Ga(a0 + i, c0 + k), hs * kac[k]);
+#pragma unroll
+            for (int l = 0; l < ND; ++l) atomicAdd(Ga(a0 + i, d0 + l), hs * kad[l]);
+        }
+    }
+    cp_async_wait<0>();
+#pragma unroll
+    for (int k = 0; k < NC; ++k)
+#pragma unroll
+        for (int l = 0; l < ND; ++l) atomicAdd(Ga(c0 + k, d0 + l), s2 * jcd[k * ND + l]);
+    if (jonly) return;
+#pragma unroll
+    for (int j = 0; j < NB; ++j)
+#pragma unroll
+        for (int k = 0; k < NC; ++k) atomicAdd(Ga(b0 + j, c0 + k), hs * kbc[j * NC + k]);
+#pragma unroll
+    for (int j = 0; j < NB; ++j)
+#pragma unroll
+        for (int l = 0; l < ND; ++l) atomicAdd(Ga(b0 + j, d0 + l), hs * kbd[j * ND + l]);
+}
+
 // Post-screen (max |e| over all roles < thr, fock_build_non_diag.f90:69) and
 // J/K scatter of a staged chunk, one thread per quartet.
 template <int NA, int NB, int NC, int ND>
@@ -346,7 +478,9 @@ __global__ void __launch_bounds__(ND_THREADS) k_scatter_staged(StagedArgs a) {
         if (!(m < a.thr)) {
             nsc = 1;
             const double s = (bra.sa == bra.sb ? 0.5 : 1.0) * (ket.sa == ket.sb ? 0.5 : 1.0);
-            scatter_strided<NA, NB, NC, ND>(a.out + t, a.stride, s, bra, ket, a.P, a.G, a.nb, a.jonly != 0);
+            extern __shared__ __align__(16) double hf_scat_smem[];
+            scatter_async<NA, NB, NC, ND>(a.out + t, a.stride, s, bra, ket, a.P, a.G, a.nb, a.jonly != 0,
+                                          hf_scat_smem);
         }
     }
     if (a.stats) warp_add_stats(a.stats, nsc, npr, a.f32 ? nsc : 0ull);
@@ -401,6 +535,7 @@ struct ClassKernels {
     int nacc, nrole_a, nrole_b;
     StagedKernel sa64[MAXR], sa32[MAXR], sb64[MAXR], sb32[MAXR], scat;
     StagedKernel dscat0, dscat1;  // staged diagonal builders (classes (X|X))
+    int scat_smem;                // dynamic shared memory of scat (bytes)
     int bi, ki, L, nout;
 };
 

@@ -666,7 +666,8 @@ __global__ void __launch_bounds__(ND_THREADS, 2) k_s2_{g.tag}_r{r}(StagedArgs a)
         reg.append(f"    k->mode = 1;\n    k->nacc = 0;\n    k->nrole_a = 0;\n    k->nrole_b = {len(roles)};")
         for r in range(len(roles)):
             reg.append(f"    k->sb64[{r}] = k_s2_{g.tag}_r{r}<false>;\n    k->sb32[{r}] = k_s2_{g.tag}_r{r}<true>;")
-        reg.append(f"    k->scat = k_scatter_staged<{NA}, {NB}, {NC}, {ND}>;")
+        reg.append(f"    k->scat = k_scatter_staged<{NA}, {NB}, {NC}, {ND}>;\n"
+                   f"    k->scat_smem = scat_smem_bytes({NA}, {NB}, {NC}, {ND});")
         if bi == ki:
             reg.append(f"    k->diag0 = nullptr;\n    k->diag1 = nullptr;")
             reg.append(f"    k->dscat0 = k_scatter_diag<{NA}, {NB}, 0>;\n    k->dscat1 = k_scatter_diag<{NA}, {NB}, 1>;")
@@ -720,7 +721,8 @@ __global__ void __launch_bounds__(ND_THREADS) k_sb_{g.tag}_r{r}(StagedArgs a) {{
             reg.append(f"    k->sa64[{r}] = k_sa_{g.tag}_r{r}<false>;\n    k->sa32[{r}] = k_sa_{g.tag}_r{r}<true>;")
         for r in range(len(outroles)):
             reg.append(f"    k->sb64[{r}] = k_sb_{g.tag}_r{r};\n    k->sb32[{r}] = k_sb_{g.tag}_r{r};")
-        reg.append(f"    k->scat = k_scatter_staged<{NA}, {NB}, {NC}, {ND}>;")
+        reg.append(f"    k->scat = k_scatter_staged<{NA}, {NB}, {NC}, {ND}>;\n"
+                   f"    k->scat_smem = scat_smem_bytes({NA}, {NB}, {NC}, {ND});")
         if bi == ki:
             reg.append(f"    k->diag0 = nullptr;\n    k->diag1 = nullptr;")
             reg.append(f"    k->dscat0 = k_scatter_diag<{NA}, {NB}, 0>;\n    k->dscat1 = k_scatter_diag<{NA}, {NB}, 1>;")

@@ -366,7 +366,7 @@ int class_index(int i, int j) {
 }
 
 struct ClassTable {
-    ClassKernels k[NCLS];
+    ClassKernels k[NCLS]{};
     ClassTable() {
         void (*reg[NCLS])(ClassKernels*) = {
             register_class_0, register_class_1, register_class_2, register_class_3, register_class_4,
@@ -374,7 +374,12 @@ struct ClassTable {
             register_class_10, register_class_11, register_class_12, register_class_13, register_class_14,
             register_class_15, register_class_16, register_class_17, register_class_18, register_class_19,
             register_class_20};
-        for (int c = 0; c < NCLS; ++c) reg[c](&k[c]);
+        for (int c = 0; c < NCLS; ++c) {
+            reg[c](&k[c]);
+            // the staged scatter streams its rows through > 48 KB of shared memory
+            if (k[c].scat && k[c].scat_smem > 0)
+                cudaFuncSetAttribute(k[c].scat, cudaFuncAttributeMaxDynamicSharedMemorySize, k[c].scat_smem);
+        }
     }
 };
 const ClassTable& class_table() {
@@ -735,7 +740,7 @@ int run_staged(hfgpu_handle* h, int c, int prec, long long n, const double* P, d
             HF_CHECK(cudaGetLastError());
         }
         ++h->launches;
-        K.scat<<<blocks, ND_THREADS, 0, stream>>>(a);
+        K.scat<<<blocks, ND_THREADS, K.scat_smem, stream>>>(a);
         HF_CHECK(cudaGetLastError());
     }
     return HFGPU_OK;
