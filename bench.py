@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the FP64-vs-mixed SCF study")
     ap.add_argument("--mixed-cutoffs", default="1e-7,1e-5")
+    ap.add_argument("--cutoff", type=float, default=0.0,
+                    help="FP32 cutoff of the timed build (0 = the FP64 build the metric is quoted on)")
     return ap.parse_args()
 
 
@@ -255,6 +257,9 @@ def run_reference(args):
                       "e2e": {"value": v, "unit": "builds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
+LLDL_DRAM_BYTES_PER_QUARTET = 2969.0  # (70 + 1500 MB read + 43 MB written) / 2 builds / 271,664 quartets
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -285,7 +290,7 @@ def main():
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
     def step():
-        fb.fock_build_device(F.data_ptr(), P.data_ptr(), THR, THR, 0.0)
+        fb.fock_build_device(F.data_ptr(), P.data_ptr(), THR, THR, args.cutoff)
 
     for _ in range(args.warmup):
         step()
@@ -343,8 +348,15 @@ def main():
     fp64_peak, fp32_peak = fock.measure_fma_peak()
     achieved = cls_flops[top] / (st["ms"][top] * 1e-3) / 1e12
     peak_tf = fp64_peak / 1e3
-    roof = {"bound": "fp64", "kernel": f"k_nondiag {fock.CLASS_NAMES[top]}", "achieved": achieved,
-            "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf, "traffic": None,
+    # DRAM bytes per LL|DL quartet (role kernels + scatter) from one ncu
+    # capture of the same kernels on C30H62 (271,664 LL|DL quartets per build;
+    # profiles/staged_class_kernels_c30h62.md), scaled by this build's count
+    traffic = None
+    if fock.CLASS_NAMES[top] == "LL|DL":
+        traffic = LLDL_DRAM_BYTES_PER_QUARTET * float(st["pass"][top])
+    roof = {"bound": "fp64", "kernel": f"class {fock.CLASS_NAMES[top]} (role kernels + k_scatter_staged)",
+            "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf,
+            "traffic": traffic, "traffic_unit": "bytes per build of the class",
             "peak_source": "measured FP64 FMA-chain probe on this device (MEASURED_PEAKS.json has no FP64 figure)",
             "all_classes_tflops": float(cls_flops.sum() / (st["ms"].sum() * 1e-3) / 1e12),
             "class_ms": {fock.CLASS_NAMES[c]: round(float(st["ms"][c]), 3) for c in range(21) if st["ms"][c] > 0},
@@ -354,7 +366,8 @@ def main():
             "class_prim_quartets": {fock.CLASS_NAMES[c]: int(st["prim"][c]) for c in range(21) if st["prim"][c] > 0}}
     out = {"metric": METRIC, "value": value, "unit": "builds/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64" if args.cutoff <= 0 else f"f64 + f32 below bound {args.cutoff:g}", "data": "synthetic",
            "config": {"workload": f"{label} one Fock build (fock_build_diag + fock_build_non_diag), thr=1e-10",
                       "nb": nb, "density": args.density, "parallelism": f"replicas{world}",
                       "l2": "flushed between steps (256 MiB write outside the timed events)"},

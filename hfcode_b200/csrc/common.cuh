@@ -348,32 +348,45 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// Shared-memory plan of the async scatter: three slab buffers when they fit
-// two blocks per SM, else two.
-__host__ __device__ constexpr int scat_nbuf(int NA, int NB, int NC, int ND) {
-    return (3 * NC * ND + NB * (NC + ND)) * ND_THREADS * 8 <= 110 * 1024 ? 3 : 2;
-}
-__host__ __device__ constexpr int scat_smem_bytes(int NA, int NB, int NC, int ND) {
-    return (scat_nbuf(NA, NB, NC, ND) * NC * ND + NB * (NC + ND)) * ND_THREADS * 8;
+template <typename E>
+__device__ __forceinline__ void cp_async_elem(E* dst, const E* src) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+    if constexpr (sizeof(E) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(src) : "memory");
 }
 
-template <int NA, int NB, int NC, int ND>
-__device__ __forceinline__ void scatter_async(const double* __restrict__ e, size_t st, double s, const GPair& bra,
+// Shared-memory plan of the async scatter (element size es): three slab
+// buffers when they fit two blocks per SM, else two.
+__host__ __device__ constexpr int scat_nbuf(int NA, int NB, int NC, int ND, int es = 8) {
+    return (3 * NC * ND + NB * (NC + ND)) * ND_THREADS * es <= 110 * 1024 ? 3 : 2;
+}
+__host__ __device__ constexpr int scat_smem_bytes(int NA, int NB, int NC, int ND, int es = 8) {
+    return (scat_nbuf(NA, NB, NC, ND, es) * NC * ND + NB * (NC + ND)) * ND_THREADS * es;
+}
+
+// E is the element type of the scratch rows and of the block sums: double
+// for FP64 quartets, float for the FP32 quartets of the mixed form (their
+// integrals are FP32 already; the sums go into G with FP64 atomics).
+template <int NA, int NB, int NC, int ND, typename E>
+__device__ __forceinline__ void scatter_async(const E* __restrict__ e, size_t st, double s, const GPair& bra,
                                               const GPair& ket, const double* __restrict__ P,
-                                              double* __restrict__ G, int nb, bool jonly, double* sm) {
-    constexpr int T = ND_THREADS, SLAB = NC * ND, NS = NA * NB, NBUF = scat_nbuf(NA, NB, NC, ND);
+                                              double* __restrict__ G, int nb, bool jonly, E* sm) {
+    constexpr int T = ND_THREADS, SLAB = NC * ND, NS = NA * NB;
+    constexpr int NBUF = scat_nbuf(NA, NB, NC, ND, (int)sizeof(E));
     const int tid = threadIdx.x;
     const int a0 = bra.aoa, b0 = bra.aob, c0 = ket.aoa, d0 = ket.aob;
-    auto Pm = [&](int r, int c) { return __ldg(P + r + (size_t)c * nb); };
+    auto Pm = [&](int r, int c) { return (E)__ldg(P + r + (size_t)c * nb); };
     auto Ga = [&](int r, int c) { return G + r + (size_t)c * nb; };
-    double* eb = sm + tid;                      // [NBUF][SLAB][T], this thread's column
-    double* pk = sm + NBUF * SLAB * T + tid;    // [NB*NC] P_bc then [NB*ND] P_bd
+    E* eb = sm + tid;                      // [NBUF][SLAB][T], this thread's column
+    E* pk = sm + NBUF * SLAB * T + tid;    // [NB*NC] P_bc then [NB*ND] P_bd
     auto issue = [&](int slab) {
         if (slab < NS) {
-            const double* src = e + (size_t)slab * SLAB * st;
-            double* dst = eb + (slab % NBUF) * SLAB * T;
+            const E* src = e + (size_t)slab * SLAB * st;
+            E* dst = eb + (slab % NBUF) * SLAB * T;
 #pragma unroll
-            for (int r = 0; r < SLAB; ++r) cp_async8(dst + r * T, src + (size_t)r * st);
+            for (int r = 0; r < SLAB; ++r) cp_async_elem(dst + r * T, src + (size_t)r * st);
         }
         cp_async_commit();  // empty groups keep the count uniform
     };
@@ -386,31 +399,31 @@ __device__ __forceinline__ void scatter_async(const double* __restrict__ e, size
 #pragma unroll
         for (int l = 0; l < ND; ++l) pk[(NB * NC + j * ND + l) * T] = Pm(b0 + j, d0 + l);
     }
-    const double s2 = 2.0 * s, hs = -0.5 * s;
-    double jcd[NC * ND], kbc[NB * NC], kbd[NB * ND], pcd[NC * ND];
+    const E s2 = (E)(2.0 * s), hs = (E)(-0.5 * s);
+    E jcd[NC * ND], kbc[NB * NC], kbd[NB * ND], pcd[NC * ND];
 #pragma unroll
-    for (int x = 0; x < NC * ND; ++x) jcd[x] = 0.0;
+    for (int x = 0; x < NC * ND; ++x) jcd[x] = 0;
 #pragma unroll
-    for (int x = 0; x < NB * NC; ++x) kbc[x] = 0.0;
+    for (int x = 0; x < NB * NC; ++x) kbc[x] = 0;
 #pragma unroll
-    for (int x = 0; x < NB * ND; ++x) kbd[x] = 0.0;
+    for (int x = 0; x < NB * ND; ++x) kbd[x] = 0;
 #pragma unroll
     for (int k = 0; k < NC; ++k)
 #pragma unroll
         for (int l = 0; l < ND; ++l) pcd[k * ND + l] = Pm(c0 + k, d0 + l);
 #pragma unroll 1
     for (int i = 0; i < NA; ++i) {
-        double jab[NB], kac[NC], kad[ND], pad_[ND], pac[NC];
+        E jab[NB], kac[NC], kad[ND], pad_[ND], pac[NC];
 #pragma unroll
-        for (int j = 0; j < NB; ++j) jab[j] = 0.0;
+        for (int j = 0; j < NB; ++j) jab[j] = 0;
 #pragma unroll
         for (int k = 0; k < NC; ++k) {
-            kac[k] = 0.0;
+            kac[k] = 0;
             pac[k] = Pm(a0 + i, c0 + k);
         }
 #pragma unroll
         for (int l = 0; l < ND; ++l) {
-            kad[l] = 0.0;
+            kad[l] = 0;
             pad_[l] = Pm(a0 + i, d0 + l);
         }
 #pragma unroll
@@ -418,14 +431,14 @@ __device__ __forceinline__ void scatter_async(const double* __restrict__ e, size
             const int slab = i * NB + j;
             issue(slab + NBUF - 1);
             cp_async_wait<NBUF - 1>();  // this thread's copies of `slab` have landed
-            const double* es = eb + (slab % NBUF) * SLAB * T;
-            const double pab = Pm(a0 + i, b0 + j);
+            const E* es = eb + (slab % NBUF) * SLAB * T;
+            const E pab = Pm(a0 + i, b0 + j);
 #pragma unroll
             for (int k = 0; k < NC; ++k) {
-                const double pbc = pk[(j * NC + k) * T];
+                const E pbc = pk[(j * NC + k) * T];
 #pragma unroll
                 for (int l = 0; l < ND; ++l) {
-                    const double v = es[(k * ND + l) * T];
+                    const E v = es[(k * ND + l) * T];
                     jab[j] += pcd[k * ND + l] * v;
                     jcd[k * ND + l] += pab * v;
                     if (!jonly) {
@@ -438,34 +451,36 @@ __device__ __forceinline__ void scatter_async(const double* __restrict__ e, size
             }
         }
 #pragma unroll
-        for (int j = 0; j < NB; ++j) atomicAdd(Ga(a0 + i, b0 + j), s2 * jab[j]);
+        for (int j = 0; j < NB; ++j) atomicAdd(Ga(a0 + i, b0 + j), (double)(s2 * jab[j]));
         if (!jonly) {
 #pragma unroll
-            for (int k = 0; k < NC; ++k) atomicAdd(Ga(a0 + i, c0 + k), hs * kac[k]);
+            for (int k = 0; k < NC; ++k) atomicAdd(Ga(a0 + i, c0 + k), (double)(hs * kac[k]));
 #pragma unroll
-            for (int l = 0; l < ND; ++l) atomicAdd(Ga(a0 + i, d0 + l), hs * kad[l]);
+            for (int l = 0; l < ND; ++l) atomicAdd(Ga(a0 + i, d0 + l), (double)(hs * kad[l]));
         }
     }
     cp_async_wait<0>();
 #pragma unroll
     for (int k = 0; k < NC; ++k)
 #pragma unroll
-        for (int l = 0; l < ND; ++l) atomicAdd(Ga(c0 + k, d0 + l), s2 * jcd[k * ND + l]);
+        for (int l = 0; l < ND; ++l) atomicAdd(Ga(c0 + k, d0 + l), (double)(s2 * jcd[k * ND + l]));
     if (jonly) return;
 #pragma unroll
     for (int j = 0; j < NB; ++j)
 #pragma unroll
-        for (int k = 0; k < NC; ++k) atomicAdd(Ga(b0 + j, c0 + k), hs * kbc[j * NC + k]);
+        for (int k = 0; k < NC; ++k) atomicAdd(Ga(b0 + j, c0 + k), (double)(hs * kbc[j * NC + k]));
 #pragma unroll
     for (int j = 0; j < NB; ++j)
 #pragma unroll
-        for (int l = 0; l < ND; ++l) atomicAdd(Ga(b0 + j, d0 + l), hs * kbd[j * ND + l]);
+        for (int l = 0; l < ND; ++l) atomicAdd(Ga(b0 + j, d0 + l), (double)(hs * kbd[j * ND + l]));
 }
 
 // Post-screen (max |e| over all roles < thr, fock_build_non_diag.f90:69) and
-// J/K scatter of a staged chunk, one thread per quartet.
-template <int NA, int NB, int NC, int ND>
-__global__ void __launch_bounds__(ND_THREADS) k_scatter_staged(StagedArgs a) {
+// J/K scatter of a staged chunk, one thread per quartet.  E is the element
+// type of the chunk's output rows (float for the FP32 chunks of staged2
+// classes in the mixed form).
+template <int NA, int NB, int NC, int ND, typename E = double>
+__global__ void __launch_bounds__(ND_THREADS, sizeof(E) == 4 ? 3 : 2) k_scatter_staged(StagedArgs a) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long nsc = 0, npr = 0;
     if (t < staged_count(a)) {
@@ -479,8 +494,8 @@ __global__ void __launch_bounds__(ND_THREADS) k_scatter_staged(StagedArgs a) {
             nsc = 1;
             const double s = (bra.sa == bra.sb ? 0.5 : 1.0) * (ket.sa == ket.sb ? 0.5 : 1.0);
             extern __shared__ __align__(16) double hf_scat_smem[];
-            scatter_async<NA, NB, NC, ND>(a.out + t, a.stride, s, bra, ket, a.P, a.G, a.nb, a.jonly != 0,
-                                          hf_scat_smem);
+            scatter_async<NA, NB, NC, ND, E>(reinterpret_cast<const E*>(a.out) + t, a.stride, s, bra, ket, a.P,
+                                             a.G, a.nb, a.jonly != 0, reinterpret_cast<E*>(hf_scat_smem));
         }
     }
     if (a.stats) warp_add_stats(a.stats, nsc, npr, a.f32 ? nsc : 0ull);
@@ -536,6 +551,8 @@ struct ClassKernels {
     StagedKernel sa64[MAXR], sa32[MAXR], sb64[MAXR], sb32[MAXR], scat;
     StagedKernel dscat0, dscat1;  // staged diagonal builders (classes (X|X))
     int scat_smem;                // dynamic shared memory of scat (bytes)
+    StagedKernel scat32;          // staged2: scatter of FP32 chunks (float rows), or nullptr
+    int scat32_smem;
     int bi, ki, L, nout;
 };
 

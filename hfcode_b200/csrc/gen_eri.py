@@ -642,11 +642,11 @@ def class_source(ci: int, bi: int, ki: int):
             code, _ = g.emit_role(f"{g.name}_r{r}", outs)
             code32, _ = g32.emit_role(f"{g32.name}_r{r}", outs)
             funcs += [code, code32]
-            stores = "\n".join(f"    {{ const double v = (double)e[{i}]; a.out[(size_t){n} * a.stride + t] = v; "
+            stores = "\n".join(f"    {{ const double v = (double)e[{i}]; out[(size_t){n} * a.stride + t] = (Real)v; "
                                f"mx = fmax(mx, fabs(v)); }}" for i, n in enumerate(outs))
             kern.append(f"""
 template <bool F32>
-__global__ void __launch_bounds__(ND_THREADS, 2) k_s2_{g.tag}_r{r}(StagedArgs a) {{
+__global__ void __launch_bounds__(ND_THREADS, F32 ? 3 : 2) k_s2_{g.tag}_r{r}(StagedArgs a) {{
     using Real = typename std::conditional<F32, float, double>::type;
     __shared__ Real sboys[BOYS_NPT * BOYS_K];
     if constexpr (F32) stage_boys<{g.L}>(sboys, a.boysf);
@@ -660,6 +660,7 @@ __global__ void __launch_bounds__(ND_THREADS, 2) k_s2_{g.tag}_r{r}(StagedArgs a)
     if constexpr (F32) eri_{g.tag}_f32_r{r}(bra, ket, a.prims, sboys, e);
     else eri_{g.tag}_r{r}(bra, ket, a.prims, sboys, e);
     double mx = 0.0;
+    Real* out = reinterpret_cast<Real*>(a.out);  // FP32 chunks keep FP32 rows
 {stores}
     a.mx[(size_t){r} * a.stride + t] = mx;
 }}""")
@@ -667,7 +668,9 @@ __global__ void __launch_bounds__(ND_THREADS, 2) k_s2_{g.tag}_r{r}(StagedArgs a)
         for r in range(len(roles)):
             reg.append(f"    k->sb64[{r}] = k_s2_{g.tag}_r{r}<false>;\n    k->sb32[{r}] = k_s2_{g.tag}_r{r}<true>;")
         reg.append(f"    k->scat = k_scatter_staged<{NA}, {NB}, {NC}, {ND}>;\n"
-                   f"    k->scat_smem = scat_smem_bytes({NA}, {NB}, {NC}, {ND});")
+                   f"    k->scat_smem = scat_smem_bytes({NA}, {NB}, {NC}, {ND});\n"
+                   f"    k->scat32 = k_scatter_staged<{NA}, {NB}, {NC}, {ND}, float>;\n"
+                   f"    k->scat32_smem = scat_smem_bytes({NA}, {NB}, {NC}, {ND}, 4);")
         if bi == ki:
             reg.append(f"    k->diag0 = nullptr;\n    k->diag1 = nullptr;")
             reg.append(f"    k->dscat0 = k_scatter_diag<{NA}, {NB}, 0>;\n    k->dscat1 = k_scatter_diag<{NA}, {NB}, 1>;")
@@ -686,7 +689,7 @@ __global__ void __launch_bounds__(ND_THREADS, 2) k_s2_{g.tag}_r{r}(StagedArgs a)
             funcs += [code, code32]
             kern.append(f"""
 template <bool F32>
-__global__ void __launch_bounds__(ND_THREADS, 2) k_sa_{g.tag}_r{r}(StagedArgs a) {{
+__global__ void __launch_bounds__(ND_THREADS, F32 ? 3 : 2) k_sa_{g.tag}_r{r}(StagedArgs a) {{
     using Real = typename std::conditional<F32, float, double>::type;
     __shared__ Real sboys[BOYS_NPT * BOYS_K];
     if constexpr (F32) stage_boys<{g.L}>(sboys, a.boysf);

@@ -379,6 +379,8 @@ struct ClassTable {
             // the staged scatter streams its rows through > 48 KB of shared memory
             if (k[c].scat && k[c].scat_smem > 0)
                 cudaFuncSetAttribute(k[c].scat, cudaFuncAttributeMaxDynamicSharedMemorySize, k[c].scat_smem);
+            if (k[c].scat32 && k[c].scat32_smem > 0)
+                cudaFuncSetAttribute(k[c].scat32, cudaFuncAttributeMaxDynamicSharedMemorySize, k[c].scat32_smem);
         }
     }
 };
@@ -740,7 +742,8 @@ int run_staged(hfgpu_handle* h, int c, int prec, long long n, const double* P, d
             HF_CHECK(cudaGetLastError());
         }
         ++h->launches;
-        K.scat<<<blocks, ND_THREADS, K.scat_smem, stream>>>(a);
+        if (prec && K.scat32) K.scat32<<<blocks, ND_THREADS, K.scat32_smem, stream>>>(a);  // float rows
+        else K.scat<<<blocks, ND_THREADS, K.scat_smem, stream>>>(a);
         HF_CHECK(cudaGetLastError());
     }
     return HFGPU_OK;
