@@ -257,7 +257,7 @@ def run_reference(args):
                       "e2e": {"value": v, "unit": "builds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
-LLDL_DRAM_BYTES_PER_QUARTET = 2969.0  # (70 + 1500 MB read + 43 MB written) / 2 builds / 271,664 quartets
+LLDL_DRAM_BYTES_PER_QUARTET = 2974.0  # (176.3 + 3750.5 MB read + 112.2 MB written) / 5 builds / 271,664 quartets
 
 
 def main():
@@ -343,7 +343,7 @@ def main():
     fb.set_timing(False)
     flops_tab = json.load(open(os.path.join(ROOT, "hfcode_b200", "csrc", "generated", "class_flops.json")))
     cls_flops = np.array([flops_tab[str(c)]["flops_prim"] * st["prim"][c] + flops_tab[str(c)]["flops_quartet"] *
-                          st["pass"][c] for c in range(21)], dtype=np.float64)
+                          st["pass"][c] for c in range(fock.NCLASS)], dtype=np.float64)
     top = int(np.argmax(st["ms"]))
     fp64_peak, fp32_peak = fock.measure_fma_peak()
     achieved = cls_flops[top] / (st["ms"][top] * 1e-3) / 1e12
@@ -359,11 +359,11 @@ def main():
             "traffic": traffic, "traffic_unit": "bytes per build of the class",
             "peak_source": "measured FP64 FMA-chain probe on this device (MEASURED_PEAKS.json has no FP64 figure)",
             "all_classes_tflops": float(cls_flops.sum() / (st["ms"].sum() * 1e-3) / 1e12),
-            "class_ms": {fock.CLASS_NAMES[c]: round(float(st["ms"][c]), 3) for c in range(21) if st["ms"][c] > 0},
+            "class_ms": {fock.CLASS_NAMES[c]: round(float(st["ms"][c]), 3) for c in range(fock.NCLASS) if st["ms"][c] > 0},
             "class_tflops": {fock.CLASS_NAMES[c]: round(float(cls_flops[c] / (st["ms"][c] * 1e-3) / 1e12), 3)
-                             for c in range(21) if st["ms"][c] > 0},
-            "class_quartets": {fock.CLASS_NAMES[c]: int(st["pass"][c]) for c in range(21) if st["pass"][c] > 0},
-            "class_prim_quartets": {fock.CLASS_NAMES[c]: int(st["prim"][c]) for c in range(21) if st["prim"][c] > 0}}
+                             for c in range(fock.NCLASS) if st["ms"][c] > 0},
+            "class_quartets": {fock.CLASS_NAMES[c]: int(st["pass"][c]) for c in range(fock.NCLASS) if st["pass"][c] > 0},
+            "class_prim_quartets": {fock.CLASS_NAMES[c]: int(st["prim"][c]) for c in range(fock.NCLASS) if st["prim"][c] > 0}}
     out = {"metric": METRIC, "value": value, "unit": "builds/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None,

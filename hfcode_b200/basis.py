@@ -246,6 +246,32 @@ def spread_basis(mol: Molecule, basis: Dict[str, ElementBasis]) -> ShellSet:
                     xyz.copy(), np.array(nbfsat, np.int32))
 
 
+def split_l_shells(sh: ShellSet, which=None) -> ShellSet:
+    """The same basis functions with L (sp) shells split into an S shell and
+    a pure P shell of the same exponents (s coefficients djk, p coefficients
+    djk * ratio), as bases such as 6-31G write them.  The AO order is
+    unchanged: the S function keeps the L shell's first AO and the P shell
+    follows it.  `which` selects the L shells to split (default: all)."""
+    cols = {k: [] for k in ("shtyp", "nzet", "atsh", "aosh", "xsh", "zeta", "djk", "djkl")}
+    for i in range(sh.nsh):
+        row = dict(shtyp=int(sh.shtyp[i]), nzet=int(sh.nzet[i]), atsh=int(sh.atsh[i]), aosh=int(sh.aosh[i]),
+                   xsh=sh.xsh[i], zeta=sh.zeta[i], djk=sh.djk[i], djkl=sh.djkl[i])
+        if row["shtyp"] == SHELL_L and (which is None or i in which):
+            srow = dict(row, shtyp=SHELL_S, djkl=np.zeros_like(sh.djkl[i]))
+            prow = dict(row, shtyp=SHELL_P, aosh=row["aosh"] + 1, djk=sh.djk[i] * sh.djkl[i],
+                        djkl=np.zeros_like(sh.djkl[i]))
+            rows = [srow, prow]
+        else:
+            rows = [row]
+        for r in rows:
+            for k in cols:
+                cols[k].append(r[k])
+    return ShellSet(np.array(cols["shtyp"], np.int32), np.array(cols["nzet"], np.int32),
+                    np.array(cols["atsh"], np.int32), np.array(cols["aosh"], np.int32),
+                    np.array(cols["xsh"], np.float64).reshape(-1, 3), np.array(cols["zeta"]),
+                    np.array(cols["djk"]), np.array(cols["djkl"]), sh.nb, sh.atcoords.copy(), sh.nbfsat.copy())
+
+
 def density_superposition(mol: Molecule, basis: Dict[str, ElementBasis], nb: int) -> np.ndarray:
     """Guess density from atomic blocks (direct_hartreefock.f90:50-59)."""
     p = np.zeros((nb, nb))

@@ -13,8 +13,14 @@
 namespace hfgpu {
 
 // ------------------------------------------------------- class traits ----
-__host__ __device__ constexpr int pt_na(int t) { return t == 0 ? 1 : t == 1 ? 4 : t == 2 ? 4 : 5; }
-__host__ __device__ constexpr int pt_nb(int t) { return t == 0 ? 1 : t == 1 ? 1 : t == 2 ? 4 : t == 3 ? 1 : t == 4 ? 4 : 5; }
+// functions of the first / second shell of pair type t
+// (SS LS LL DS DL DD PS LP PP DP)
+__host__ __device__ constexpr int pt_na(int t) {
+    return t == 0 ? 1 : t <= 2 ? 4 : t <= 5 ? 5 : t == 6 ? 3 : t == 7 ? 4 : t == 8 ? 3 : 5;
+}
+__host__ __device__ constexpr int pt_nb(int t) {
+    return t == 0 || t == 1 || t == 3 || t == 6 ? 1 : t == 2 || t == 4 ? 4 : t == 5 ? 5 : 3;
+}
 
 #define HF_CLASS_TRAITS(ci, bi, ki, NAME, nout, L)                                                   \
     struct Cls_##NAME {                                                                              \

@@ -41,15 +41,20 @@ LMAX = {"S": 0, "L": 1, "D": 2, "P": 1}
 SUBS = {"S": [(0, False)], "L": [(0, False), (1, True)], "D": [(2, False)], "P": [(1, False)]}
 
 # GPU pair types (larger shell first) and the quartet classes over {S,L,D}
-PAIR_TYPES = [("S", "S"), ("L", "S"), ("L", "L"), ("D", "S"), ("D", "L"), ("D", "D")]
+# GPU pair types, larger shell first (D > L > P > S); the four with pure p
+# shells come last so the classes of the {s, l, d} bases keep indices 0..20
+PAIR_TYPES = [("S", "S"), ("L", "S"), ("L", "L"), ("D", "S"), ("D", "L"), ("D", "D"),
+              ("P", "S"), ("L", "P"), ("P", "P"), ("D", "P")]
+N_SLD_TYPES = 6
 PAIR_NAMES = ["".join(p) for p in PAIR_TYPES]
 
 
 def class_list():
-    out = []
-    for i in range(len(PAIR_TYPES)):
-        for j in range(i, len(PAIR_TYPES)):
-            out.append((i, j))
+    """Quartet classes (bra type <= ket type): the 21 classes over the
+    {s, l, d} pair types first, then every class with a pure-p pair type."""
+    n = len(PAIR_TYPES)
+    out = [(i, j) for i in range(N_SLD_TYPES) for j in range(i, N_SLD_TYPES)]
+    out += [(i, j) for i in range(n) for j in range(i, n) if j >= N_SLD_TYPES]
     return out
 
 
@@ -315,6 +320,8 @@ class ClassGen:
         w("        const GPrim pb = load_prim(prims, bra.p0 + ib * bra.ps);")
         w(f"        const {ft} p = {cv('pb.p')};")
         w(f"        const {ft} PA0 = {cv('pb.P[0] - Ax')}, PA1 = {cv('pb.P[1] - Ay')}, PA2 = {cv('pb.P[2] - Az')};")
+        if L > 0:
+            w(f"        const {ft} h2p1 = {'0.5' if dbl else '0.5f'} / p;  // bra-only, out of the ket loop")
         used_b = sorted({k[0] for k in acc})
         used_k = sorted({k[1] for k in acc})
         for bi in used_b:
@@ -326,7 +333,10 @@ class ClassGen:
         w(f"            const {ft} q = {cv('pk.p')};")
         one = "1.0" if dbl else "1.0f"
         half = "0.5" if dbl else "0.5f"
-        w(f"            const {ft} opq = {one} / (p + q);")
+        # one reciprocal square root per primitive quartet gives both
+        # 1/(p+q) and the sqrt(1/(p+q)) of the prefactor
+        w(f"            const {ft} rs = {'rsqrt' if dbl else 'rsqrtf'}(p + q);")
+        w(f"            const {ft} opq = rs * rs;")
         w(f"            const {ft} rho = p * q * opq;")
         if dbl:
             w("            const double PQ0 = pb.P[0] - pk.P[0], PQ1 = pb.P[1] - pk.P[1], PQ2 = pb.P[2] - pk.P[2];")
@@ -337,9 +347,9 @@ class ClassGen:
         w(f"            {ft} F[{L + 1}];")
         w(f"            boys_eval<{L}>(T, btab, F);")
         if dbl:
-            w("            const double pref = pb.K * pk.K * sqrt(opq);")
+            w("            const double pref = pb.K * pk.K * rs;")
         else:
-            w("            const float pref = (float)(pb.K * pk.K) * sqrtf(opq);")
+            w("            const float pref = (float)(pb.K * pk.K) * rs;")
         for m in range(L + 1):
             w(f"            const {ft} B{m} = pref * F[{m}];")
         if L > 0:
@@ -351,8 +361,8 @@ class ClassGen:
             else:
                 w("            const float QC0 = (float)(pk.P[0] - Cx), QC1 = (float)(pk.P[1] - Cy), "
                   "QC2 = (float)(pk.P[2] - Cz);")
-            w(f"            const {ft} h2p1 = {half} / p, rp = rho / p;")
-            w(f"            const {ft} h2q1 = {half} / q, rq = rho / q;")
+            w(f"            const {ft} rp = qo, rq = po;  // rho/p = q/(p+q), rho/q = p/(p+q)")
+            w(f"            const {ft} h2q1 = {half} / q;")
             w(f"            const {ft} h2pq1 = {half} * opq;")
             for n in range(2, 5):
                 w(f"            const {ft} h2p{n} = {n} * h2p1, h2q{n} = {n} * h2q1, h2pq{n} = {n} * h2pq1;")
@@ -895,6 +905,18 @@ def main(outdir: str):
     inc = '#include "../scatter.cuh"\n'
     inc += "".join(f'#include "cls_{ci:02d}_{info["tag"]}.cuh"\n' for ci, info in flops.items())
     inc += "namespace hfgpu {\n#include \"host_dispatch.inc\"\n}\n"
+    cl = class_list()
+    tab = ["// GENERATED by gen_eri.py -- quartet classes over the GPU pair types.",
+           f"#define HF_NPT {len(PAIR_TYPES)}",
+           f"#define HF_NCLS {len(cl)}",
+           "#define HF_CLASS_BI_LIST " + ", ".join(str(b) for b, _ in cl),
+           "#define HF_CLASS_KI_LIST " + ", ".join(str(k) for _, k in cl),
+           "#define HF_FOR_EACH_CLASS(X) " + " ".join(f"X({c})" for c in range(len(cl))),
+           "#define HF_PAIR_NAMES " + ", ".join(f'"{a}{b}"' for a, b in PAIR_TYPES), ""]
+    ct = os.path.join(outdir, "class_table.inc")
+    if not os.path.exists(ct) or open(ct).read() != "\n".join(tab):
+        with open(ct, "w") as fh:
+            fh.write("\n".join(tab))
     ai = os.path.join(outdir, "all_classes.inc")
     if not os.path.exists(ai) or open(ai).read() != inc:
         with open(ai, "w") as fh:

@@ -40,14 +40,14 @@
 
 #include "../../include/hfgpu.h"
 #include "common.cuh"
+#include "generated/class_table.inc"
 #include "pairs.hpp"
 
 namespace hfgpu {
 #define HF_DECL_REG(ci) void register_class_##ci(ClassKernels* k);
-HF_DECL_REG(0) HF_DECL_REG(1) HF_DECL_REG(2) HF_DECL_REG(3) HF_DECL_REG(4) HF_DECL_REG(5) HF_DECL_REG(6)
-HF_DECL_REG(7) HF_DECL_REG(8) HF_DECL_REG(9) HF_DECL_REG(10) HF_DECL_REG(11) HF_DECL_REG(12) HF_DECL_REG(13)
-HF_DECL_REG(14) HF_DECL_REG(15) HF_DECL_REG(16) HF_DECL_REG(17) HF_DECL_REG(18) HF_DECL_REG(19) HF_DECL_REG(20)
+HF_FOR_EACH_CLASS(HF_DECL_REG)
 #undef HF_DECL_REG
+static_assert(HF_NPT == NPT && HF_NCLS == NCLS, "generated class table out of date");
 }  // namespace hfgpu
 
 using namespace hfgpu;
@@ -76,8 +76,8 @@ std::recursive_mutex g_dev_mu;
 constexpr double SHTHRESH = 1e-11;      // molprops.f90:163
 constexpr int NSTREAM = 4;              // concurrent class streams of the off-diagonal build
 // bra and ket pair types of the 21 quartet classes (pair types i <= j, row by row)
-__constant__ int CLS_BI[NCLS] = {0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 1, 2, 2, 2, 2, 3, 3, 3, 4, 4, 5};
-__constant__ int CLS_KI[NCLS] = {0, 1, 2, 3, 4, 5, 1, 2, 3, 4, 5, 2, 3, 4, 5, 3, 4, 5, 4, 5, 5};
+__constant__ int CLS_BI[NCLS] = {HF_CLASS_BI_LIST};
+__constant__ int CLS_KI[NCLS] = {HF_CLASS_KI_LIST};
 
 // evaluate_maxdm.f90: one thread per unordered shell pair.
 __global__ void k_maxdm(const int* __restrict__ shtyp, const int* __restrict__ aosh, int nsh, int nb,
@@ -356,24 +356,20 @@ int dalloc(T** p, size_t n) {
     return HFGPU_OK;
 }
 
-// class index of pair types (i <= j), enumerated row by row
+// class index of pair types (i <= j) in the generator's class order
 int class_index(int i, int j) {
-    int c = 0;
-    for (int a = 0; a < NPT; ++a)
-        for (int b = a; b < NPT; ++b, ++c)
-            if (a == i && b == j) return c;
+    static const int bi[NCLS] = {HF_CLASS_BI_LIST}, ki[NCLS] = {HF_CLASS_KI_LIST};
+    for (int c = 0; c < NCLS; ++c)
+        if (bi[c] == i && ki[c] == j) return c;
     return -1;
 }
 
 struct ClassTable {
     ClassKernels k[NCLS]{};
     ClassTable() {
-        void (*reg[NCLS])(ClassKernels*) = {
-            register_class_0, register_class_1, register_class_2, register_class_3, register_class_4,
-            register_class_5, register_class_6, register_class_7, register_class_8, register_class_9,
-            register_class_10, register_class_11, register_class_12, register_class_13, register_class_14,
-            register_class_15, register_class_16, register_class_17, register_class_18, register_class_19,
-            register_class_20};
+#define HF_REG_PTR(ci) register_class_##ci,
+        void (*reg[NCLS])(ClassKernels*) = {HF_FOR_EACH_CLASS(HF_REG_PTR)};
+#undef HF_REG_PTR
         for (int c = 0; c < NCLS; ++c) {
             reg[c](&k[c]);
             // the staged scatter streams its rows through > 48 KB of shared memory
@@ -785,7 +781,7 @@ int run_non_diag(hfgpu_handle* h, const double* P, double thr, int jonly, double
         k_screen<0><<<blocks, 256, 0, h->stream>>>(sa);  // survivors per sub-class
         HF_CHECK(cudaGetLastError());
         ++h->launches;
-        k_offsets<<<1, 32, 0, h->stream>>>(h->offs, h->d_subs, h->d_cnt, h->d_ncls);
+        k_offsets<<<1, (NCLS + 31) / 32 * 32, 0, h->stream>>>(h->offs, h->d_subs, h->d_cnt, h->d_ncls);
         HF_CHECK(cudaGetLastError());
         HF_CHECK(cudaMemsetAsync(h->d_cnt, 0, cbytes, h->stream));
         ++h->launches;
@@ -897,9 +893,9 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
     const int MP = B->maxprim;
     for (int s = 0; s < h->nsh; ++s) {
         int t = h->shtyp[s];
-        if (t != HFGPU_SHELL_S && t != HFGPU_SHELL_D && t != HFGPU_SHELL_L) {
+        if (t != HFGPU_SHELL_S && t != HFGPU_SHELL_P && t != HFGPU_SHELL_D && t != HFGPU_SHELL_L) {
             delete h;
-            return set_err(HFGPU_ERR_UNSUPPORTED, "hfgpu_init: pure p shells are not supported by the GPU classes");
+            return set_err(HFGPU_ERR_ARG, "hfgpu_init: unknown shell type " + std::to_string(t));
         }
         if (h->nzet[s] < 1 || h->nzet[s] > MP) {
             delete h;

@@ -26,7 +26,7 @@ inline int ref_class(int r1, int r2) {
     return tab[r1][r2];
 }
 // GPU pair type of a reference class, and whether the GPU pair swaps the
-// reference's (first, second) order; -1 for classes with pure p shells.
+// reference's (first, second) order (the GPU puts the larger shell first).
 inline int gpu_type_of_ref(int rc, bool* swap) {
     switch (rc) {
         case 0: *swap = false; return 0;  // ss -> SS
@@ -35,10 +35,14 @@ inline int gpu_type_of_ref(int rc, bool* swap) {
         case 2: *swap = true; return 3;   // sd -> DS
         case 8: *swap = false; return 4;  // dl -> DL
         case 7: *swap = false; return 5;  // dd -> DD
+        case 1: *swap = true; return 6;   // sp -> PS
+        case 6: *swap = true; return 7;   // pl -> LP
+        case 4: *swap = false; return 8;  // pp -> PP
+        case 5: *swap = true; return 9;   // pd -> DP
         default: *swap = false; return -1;
     }
 }
-constexpr int GPU_TO_REF[NPT] = {0, 3, 9, 2, 8, 7};
+constexpr int GPU_TO_REF[NPT] = {0, 3, 9, 2, 8, 7, 1, 6, 4, 5};
 
 // One shell pair in GPU orientation with its surviving primitive pairs
 // appended to prims: K_ab = sqrt(2 pi^2.5) exp(-ab/p r^2)/p d_a d_b, dropped

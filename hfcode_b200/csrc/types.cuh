@@ -9,8 +9,8 @@
 namespace hfgpu {
 
 constexpr double INTTHRESH = 1e-10;     // molprops.f90:162
-constexpr int NPT = 6;                  // GPU pair types SS LS LL DS DL DD
-constexpr int NCLS = 21;                // quartet classes over the pair types
+constexpr int NPT = 10;                 // GPU pair types SS LS LL DS DL DD PS LP PP DP
+constexpr int NCLS = 55;                // quartet classes over the pair types (21 without pure p)
 constexpr int BOYS_NPT = 225;           // grid T_j = j/8, j = 0..224 (T <= 28)
 constexpr int BOYS_K = 8;               // Taylor terms per grid point
 constexpr int BOYS_MMAX = 8;            // highest order used: (dd|dd)

@@ -27,8 +27,13 @@ from .cabi import BasisDescriptor
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(_HERE, "libhfgpu.so")
 
-CLASS_NAMES = [f"{a}|{b}" for i, a in enumerate(["SS", "LS", "LL", "DS", "DL", "DD"])
-               for b in ["SS", "LS", "LL", "DS", "DL", "DD"][i:]]
+# GPU pair types and quartet classes in the order of include/hfgpu.h
+# (HFGPU_NCLASS): the 21 classes over the {s, l, d} types, then every class
+# with a pure-p type
+PAIR_TYPES = ["SS", "LS", "LL", "DS", "DL", "DD", "PS", "LP", "PP", "DP"]
+CLASS_NAMES = ([f"{PAIR_TYPES[i]}|{PAIR_TYPES[j]}" for i in range(6) for j in range(i, 6)] +
+               [f"{PAIR_TYPES[i]}|{PAIR_TYPES[j]}" for i in range(10) for j in range(i, 10) if j >= 6])
+NCLASS = len(CLASS_NAMES)
 REF_CLASSES = ["ss", "sp", "sd", "sl", "pp", "pd", "pl", "dd", "dl", "ll"]
 
 
@@ -225,8 +230,8 @@ class FockBuilder:
         return s, dict(zip(REF_CLASSES, list(last)))
 
     def class_stats(self) -> Dict[str, np.ndarray]:
-        arrs = [(ctypes.c_longlong * 21)() for _ in range(4)]
-        ms = (ctypes.c_double * 21)()
+        arrs = [(ctypes.c_longlong * NCLASS)() for _ in range(4)]
+        ms = (ctypes.c_double * NCLASS)()
         _check(_lib.hfgpu_get_class_stats(self.h, *arrs, ms), "get_class_stats")
         keys = ["pass", "scattered", "prim", "fp32"]
         out = {k: np.array(list(a), dtype=np.int64) for k, a in zip(keys, arrs)}

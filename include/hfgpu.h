@@ -125,11 +125,15 @@ int hfgpu_dims(const hfgpu_handle* h, int* nb, int* nsh, int* npairs);
  * ss, sp, sd, sl, pp, pd, pl, dd, dl, ll (index_sort.f90:95-119). */
 int hfgpu_get_schwarz(const hfgpu_handle* h, double* schw_sh, int* last);
 
-/* Statistics of the last off-diagonal build, per quartet class (21 classes
- * over the pair types SS, LS, LL, DS, DL, DD; class c pairs types (i,j),
- * i <= j, enumerated row by row): screened-in shell quartets, quartets that
- * passed the max|e| post-screen, primitive quartets evaluated, FP32 quartets
- * (mixed form), and the kernel time in ms (0 unless timing is enabled). */
+/* Statistics of the last off-diagonal build, per quartet class: arrays of
+ * HFGPU_NCLASS entries.  The GPU pair types are SS LS LL DS DL DD PS LP PP DP
+ * (larger shell first); classes 0..20 pair the first six types (i <= j, row
+ * by row), classes 21..54 every pair of types that involves a pure p type
+ * (i <= j, row by row, j >= 6).  Per class: screened-in shell quartets,
+ * quartets that passed the max|e| post-screen, primitive quartets evaluated,
+ * FP32 quartets (mixed form), and the kernel time in ms (0 unless timing is
+ * enabled). */
+#define HFGPU_NCLASS 55
 int hfgpu_get_class_stats(const hfgpu_handle* h, long long* n_pass, long long* n_scattered,
                           long long* n_prim, long long* n_fp32, double* ms);
 

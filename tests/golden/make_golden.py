@@ -5,6 +5,8 @@
 energies.json   converged RHF energies (direct_hartreefock protocol, conve 1e-10,
                 conv 1e-7, atomic-density guess) of water/STO-3G, CH4 and
                 benzene/6-31G(d), spherical d as the reference.
+"_sp" systems   the same molecules with every L shell split into S + pure P
+                (hfcode_b200.basis.split_l_shells): the pure-p classes.
 fock_*.npz      F = fock_build_initial_diag + fock_build_non_diag at the
                 atomic-density guess, thr 1e-10, F starting at zero.
 The reference publishes no outputs, so these pin the oracle against itself
@@ -24,7 +26,7 @@ from helpers import system  # noqa: E402
 from hfcode_b200 import scf  # noqa: E402
 from oracle import pyoracle  # noqa: E402
 
-SYSTEMS = ["water", "alkane1", "benzene"]
+SYSTEMS = ["water", "alkane1", "benzene", "water_sp", "benzene_sp"]
 
 
 def main():

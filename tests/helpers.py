@@ -10,6 +10,19 @@ from hfcode_b200 import basis, molecules
 
 @functools.lru_cache(maxsize=None)
 def system(name: str):
+    """(molecule, basis, shells, guess density).  A "_sp" suffix splits every
+    L shell into S + pure P (same functions, pure-p quartet classes); "_mix"
+    splits every other L shell, so S, P, D and L shells coexist."""
+    if name.endswith("_sp") or name.endswith("_mix"):
+        base, kind = name.rsplit("_", 1)
+        mol, bas, sh, p0 = system(base)
+        ls = [i for i in range(sh.nsh) if sh.shtyp[i] == basis.SHELL_L]
+        which = None if kind == "sp" else set(ls[::2])
+        return mol, bas, basis.split_l_shells(sh, which), p0
+    return _system(name)
+
+
+def _system(name: str):
     if name == "water":
         mol, bas = molecules.water(), basis.load_basis("STO-3G")
     elif name == "benzene":

@@ -15,6 +15,8 @@
 static inline int __double2int_rn(double x) { return (int)std::nearbyint(x); }
 static inline int __float2int_rn(float x) { return (int)std::nearbyintf(x); }
 #define __expf(x) std::exp((float)(x))
+static inline double rsqrt(double x) { return 1.0 / std::sqrt(x); }
+static inline float rsqrtf(float x) { return 1.0f / std::sqrt(x); }
 template <class T>
 static inline T __ldg(const T* p) { return *p; }
 static inline double atomicAdd(double* p, double v) {

@@ -23,8 +23,16 @@ from oracle import pyoracle
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(ROOT, "hfcode_b200", "csrc")
 GEN = os.path.join(CSRC, "generated")
-TYPES = {1: "S", 12: "L", 3: "D"}
-PAIR_TYPES = [("S", "S"), ("L", "S"), ("L", "L"), ("D", "S"), ("D", "L"), ("D", "D")]
+TYPES = {1: "S", 2: "P", 12: "L", 3: "D"}
+NFUNC = {1: 1, 2: 3, 12: 4, 3: 5}
+
+
+def _gen():
+    import sys
+    sys.path.insert(0, CSRC)
+    import gen_eri
+    sys.path.pop(0)
+    return gen_eri
 
 
 def _build():
@@ -65,29 +73,24 @@ def _dp(a):
 
 
 def class_quartets(sh, rng, n=3):
-    """Shell quartets of every class in GPU orientation."""
+    """Shell quartets of every generated class in GPU orientation."""
+    g = _gen()
     by = {t: [int(i) for i in np.where(sh.shtyp == c)[0]] for c, t in TYPES.items()}
     out = {}
-    ci = 0
-    for bi in range(6):
-        for ki in range(bi, 6):
-            qs = []
-            for _ in range(n):
-                A, B = PAIR_TYPES[bi]
-                C, D = PAIR_TYPES[ki]
-                qs.append(tuple(int(rng.choice(by[x])) for x in (A, B, C, D)))
-            # one quartet with the same pair twice (the diagonal builders' case)
-            if bi == ki:
-                q = qs[0]
-                qs.append((q[0], q[1], q[0], q[1]))
-            out[ci] = qs
-            ci += 1
+    for ci, (bi, ki) in enumerate(g.class_list()):
+        A, B = g.PAIR_TYPES[bi]
+        C, D = g.PAIR_TYPES[ki]
+        qs = [tuple(int(rng.choice(by[x])) for x in (A, B, C, D)) for _ in range(n)]
+        if bi == ki:  # one quartet with the same pair twice (the diagonal builders' case)
+            q = qs[0]
+            qs.append((q[0], q[1], q[0], q[1]))
+        out[ci] = qs
     return out
 
 
 def test_generated_eri_matches_oracle(host):
     lib, info = host
-    _, _, sh, _ = system("alkane2")
+    _, _, sh, _ = system("alkane2_mix")  # S, P, D and L shells: every class
     desc = BasisDescriptor(sh)
     h = lib.hc_create(ctypes.addressof(desc.struct))
     orc = pyoracle.Oracle(sh)
@@ -108,7 +111,7 @@ def test_generated_eri_matches_oracle(host):
 
 def test_generated_scatter_matches_uniform_scatter(host):
     lib, info = host
-    _, _, sh, _ = system("alkane2")
+    _, _, sh, _ = system("alkane2_mix")
     desc = BasisDescriptor(sh)
     h = lib.hc_create(ctypes.addressof(desc.struct))
     orc = pyoracle.Oracle(sh)
@@ -120,7 +123,7 @@ def test_generated_scatter_matches_uniform_scatter(host):
     for ci, qs in class_quartets(sh, rng, n=2).items():
         for q in qs:
             e = orc.eri(*q)
-            na, nb_, nc, nd = (4 if sh.shtyp[s] == 12 else 5 if sh.shtyp[s] == 3 else 1 for s in q)
+            na, nb_, nc, nd = (NFUNC[int(sh.shtyp[s])] for s in q)
             E = e.reshape(na, nb_, nc, nd)
             for jonly in (0, 1):
                 s = 0.25

@@ -12,7 +12,7 @@ from oracle import pyoracle
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
-@pytest.mark.parametrize("name", ["water", "alkane1", "benzene"])
+@pytest.mark.parametrize("name", ["water", "alkane1", "benzene", "water_sp", "benzene_sp"])
 def test_oracle_fock_matches_golden(name):
     _, _, sh, p0 = system(name)
     orc = pyoracle.Oracle(sh)
@@ -23,7 +23,7 @@ def test_oracle_fock_matches_golden(name):
     assert np.max(np.abs(f - ref)) < 1e-12
 
 
-@pytest.mark.parametrize("name", ["water", "alkane1"])
+@pytest.mark.parametrize("name", ["water", "alkane1", "water_sp"])
 def test_oracle_scf_energy_matches_golden(name):
     gold = json.load(open(os.path.join(GOLD, "energies.json")))[name]
     mol, _, sh, p0 = system(name)

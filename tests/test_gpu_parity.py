@@ -11,22 +11,21 @@ from helpers import perturbed_density, system
 from oracle import pyoracle
 
 TOL = 1e-10
-REF2GPU = {0: 0, 3: 1, 9: 2, 2: 3, 8: 4, 7: 5}  # ss sl ll sd dl dd -> SS LS LL DS DL DD
+# reference pair classes (ss sp sd sl pp pd pl dd dl ll) -> GPU pair types
+# (SS LS LL DS DL DD PS LP PP DP)
+REF2GPU = {0: 0, 3: 1, 9: 2, 2: 3, 8: 4, 7: 5, 1: 6, 6: 7, 4: 8, 5: 9}
 
 
 def gpu_class(ti, tj):
+    from hfcode_b200.fock import CLASS_NAMES, PAIR_TYPES
     a, b = min(ti, tj), max(ti, tj)
-    c = 0
-    for i in range(6):
-        for j in range(i, 6):
-            if (i, j) == (a, b):
-                return c
-            c += 1
+    return CLASS_NAMES.index(f"{PAIR_TYPES[a]}|{PAIR_TYPES[b]}")
 
 
 def oracle_counts_by_gpu_class(orc):
     passed, _ = orc.counts()
-    out = np.zeros(21, dtype=np.int64)
+    from hfcode_b200.fock import NCLASS
+    out = np.zeros(NCLASS, dtype=np.int64)
     for ca in range(10):
         for cb in range(10):
             if passed[ca, cb]:
@@ -35,7 +34,7 @@ def oracle_counts_by_gpu_class(orc):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["water", "alkane1", "alkane2", "benzene"])
+@pytest.mark.parametrize("name", ["water", "alkane1", "alkane2", "benzene", "water_sp", "alkane2_sp", "alkane2_mix"])
 def test_fock_build_parity(name):
     from hfcode_b200.fock import FockBuilder
     _, _, sh, p0 = system(name)
