@@ -25,6 +25,7 @@ from __future__ import annotations
 import argparse
 import dataclasses
 import json
+import os
 import queue
 import threading
 import time
@@ -87,7 +88,7 @@ def estimate_footprint(sh: ShellSet, scratch_budget: int) -> int:
 class Server:
     def __init__(self, hbm_budget: int, max_slots: int = 8, scratch_budget: int = 256 << 20,
                  fp32_cutoff: float = 1e-7, conve: float = 1e-8, conv: float = 1e-6, basis_name: str = "6-31G(d)",
-                 graphs: bool = True):
+                 graphs: bool = False):
         from . import fock  # loads the CUDA library; fails loudly without it
         self.fock = fock
         self.hbm_budget = hbm_budget
@@ -95,7 +96,12 @@ class Server:
         self.scratch_budget = scratch_budget
         self.fp32_cutoff = fp32_cutoff
         self.conve, self.conv = conve, conv
-        self.graphs = graphs  # builds after the first as CUDA-graph replays
+        # builds after the first as CUDA-graph replays; off by default: a
+        # served SCF changes its thresholds four times in ~15 cycles, so each
+        # job records four graphs for ~13 replays, and the recordings (taken
+        # under the library's device lock) cost more than the launches they
+        # save (measured 7.8 vs 11.9 jobs/s, 200 jobs, 8 slots)
+        self.graphs = graphs
         self.basis = basismod.load_basis(basis_name)
         self.lock = threading.Condition()
         self.in_use = 0
@@ -162,9 +168,22 @@ class Server:
             job.finished = time.perf_counter() - t0
             self._release(job.footprint)
 
+    @property
+    def blas_threads(self) -> int:
+        """Host BLAS/LAPACK threads: the cores shared among the slots.  Every
+        job's SCF step calls LAPACK from its own thread; letting each call
+        use all cores oversubscribes the host (measured 3.4 -> 10.7 jobs/s
+        on a 16-core host with 8 slots when limited to 2 threads)."""
+        return max(1, (os.cpu_count() or 1) // self.max_slots)
+
     def serve(self, jobs: List[Job], realtime: bool = True) -> Dict:
         """Runs the stream; each job is released at its arrival time (or all
         at once with realtime=False) and admitted FIFO."""
+        from threadpoolctl import threadpool_limits
+        with threadpool_limits(limits=self.blas_threads):
+            return self._serve(jobs, realtime)
+
+    def _serve(self, jobs: List[Job], realtime: bool) -> Dict:
         for j in jobs:
             self.prepare(j)
         t0 = time.perf_counter()
@@ -204,6 +223,12 @@ class Server:
 
 def serve_sequential(jobs: List[Job], server: Server) -> Dict:
     """The plain per-job form: one job at a time on the GPU, same protocol."""
+    from threadpoolctl import threadpool_limits
+    with threadpool_limits(limits=server.blas_threads):
+        return _serve_sequential(jobs, server)
+
+
+def _serve_sequential(jobs: List[Job], server: Server) -> Dict:
     for j in jobs:
         server.prepare(j)
     t0 = time.perf_counter()
@@ -229,17 +254,17 @@ def main():
     ap.add_argument("--hbm-gb", type=float, default=64.0)
     ap.add_argument("--fp32-cutoff", type=float, default=1e-7)
     ap.add_argument("--sequential", action="store_true", help="also run the plain per-job form")
-    ap.add_argument("--no-graphs", action="store_true", help="separate diag / non-diag calls per build")
+    ap.add_argument("--graphs", action="store_true", help="builds after the first as CUDA-graph replays")
     args = ap.parse_args()
     srv = Server(int(args.hbm_gb * (1 << 30)), args.slots, fp32_cutoff=args.fp32_cutoff,
-                 graphs=not args.no_graphs)
+                 graphs=args.graphs)
     jobs = make_stream(args.jobs, args.rate)
     out = {"served": srv.serve(jobs)}
     if args.sequential:
         seq = make_stream(args.jobs, args.rate)
         out["sequential"] = serve_sequential(seq, Server(int(args.hbm_gb * (1 << 30)), 1,
                                                         fp32_cutoff=args.fp32_cutoff,
-                                                        graphs=not args.no_graphs))
+                                                        graphs=args.graphs))
     print(json.dumps(out))
 
 

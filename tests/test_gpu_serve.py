@@ -9,10 +9,11 @@ import pytest
 
 
 @pytest.mark.gpu
-def test_served_results_match_alone():
+@pytest.mark.parametrize("graphs", [False, True])
+def test_served_results_match_alone(graphs):
     from hfcode_b200 import serve
     jobs_mix = serve.make_stream(10, rate=0.0, seed=4242, max_alkane=5, max_water=4)
-    srv = serve.Server(hbm_budget=32 << 30, max_slots=4, fp32_cutoff=1e-7)
+    srv = serve.Server(hbm_budget=32 << 30, max_slots=4, fp32_cutoff=1e-7, graphs=graphs)
     out = srv.serve(jobs_mix, realtime=False)
     assert out["failed"] == 0 and out["not_converged"] == 0, out["errors"]
     assert 1 <= srv.peak_active <= 4
