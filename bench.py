@@ -172,6 +172,18 @@ def mixed_study(fock, mol, sh, cutoffs, dev):
     r64 = scf.direct_hartreefock(mol, sh, fb, p_guess=p0, conve=1e-9, conv=1e-6, maxiter=80, ints=ints)
     out["scf_fp64"] = {"energy": r64.energy, "cycles": r64.cycles, "converged": r64.converged,
                        "seconds": time.perf_counter() - t0}
+    # the same SCF with every cycle on the device (CUDA-graph replays, SP2
+    # density), FP64 and mixed in the incremental builds
+    from hfcode_b200.device_scf import DeviceSCF
+    for label, cut in (("device_scf_fp64", 0.0), ("device_scf_mixed_1e-05", 1e-5)):
+        fbd = fock.FockBuilder(sh)
+        t1 = time.perf_counter()
+        rd = DeviceSCF(mol, sh, fbd, ints=ints).run(p0, conve=1e-9, conv=1e-6, maxiter=80, fp32_cutoff=cut)
+        sec = time.perf_counter() - t1
+        fbd.close()
+        out[label] = {"energy": rd.energy, "cycles": rd.cycles, "converged": rd.converged, "seconds": sec,
+                      "abs_dE_vs_host_fp64": abs(rd.energy - r64.energy),
+                      "scf_builds_per_s": rd.cycles / sec}
     # a delta-P near convergence: the converged density against the core-free
     # one-cycle update (P_next - P), the size the incremental builds see late
     nb = sh.nb

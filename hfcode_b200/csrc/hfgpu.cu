@@ -1166,6 +1166,57 @@ int hfgpu_graph_launch(hfgpu_handle* h) {
     return HFGPU_OK;
 }
 
+// Enqueue one device build on the caller's stream with no host round trip
+// (launches sized as for a capture), so that a caller's own CUDA-graph
+// capture of a whole SCF iteration can include it.
+int hfgpu_fock_build_device_on(hfgpu_handle* h, double* f_dev, const double* p_dev, double thr_diag,
+                               double thr_non_diag, double fp32_cutoff, void* stream) {
+    if (!h || !f_dev || !p_dev) return set_err(HFGPU_ERR_ARG, "null argument");
+    if (!h->have_schwarz) return set_err(HFGPU_ERR_STATE, "fock_build_initial_diag has not been called");
+    cudaStream_t own = h->stream;
+    h->stream = (cudaStream_t)stream;  // the build forks from and joins back to this stream
+    const int rc = device_build(h, f_dev, p_dev, thr_diag, thr_non_diag, fp32_cutoff, true);
+    h->stream = own;
+    return rc;
+}
+
+// Solves the (n x n) system A x = b in place of b on the device (Gaussian
+// elimination with partial pivoting, one thread): the DIIS equations of a
+// device-resident SCF step, n <= 32.  A is row-major and is overwritten.
+__global__ void k_small_solve(double* A, double* b, int n, int* status) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int ok = 1;
+    for (int c = 0; c < n; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < n; ++r)
+            if (fabs(A[r * n + c]) > fabs(A[piv * n + c])) piv = r;
+        if (A[piv * n + c] == 0.0) { ok = 0; break; }
+        if (piv != c) {
+            for (int k = 0; k < n; ++k) { const double t = A[c * n + k]; A[c * n + k] = A[piv * n + k]; A[piv * n + k] = t; }
+            const double t = b[c]; b[c] = b[piv]; b[piv] = t;
+        }
+        for (int r = c + 1; r < n; ++r) {
+            const double m = A[r * n + c] / A[c * n + c];
+            for (int k = c; k < n; ++k) A[r * n + k] -= m * A[c * n + k];
+            b[r] -= m * b[c];
+        }
+    }
+    if (ok)
+        for (int r = n - 1; r >= 0; --r) {
+            double s = b[r];
+            for (int k = r + 1; k < n; ++k) s -= A[r * n + k] * b[k];
+            b[r] = s / A[r * n + r];
+        }
+    if (status) *status = ok;
+}
+
+int hfgpu_small_solve(double* a_dev, double* b_dev, int n, int* status_dev, void* stream) {
+    if (!a_dev || !b_dev || n <= 0 || n > 32) return set_err(HFGPU_ERR_ARG, "hfgpu_small_solve: bad arguments");
+    k_small_solve<<<1, 32, 0, (cudaStream_t)stream>>>(a_dev, b_dev, n, status_dev);
+    HF_CHECK(cudaGetLastError());
+    return HFGPU_OK;
+}
+
 int hfgpu_fock_build_graph(hfgpu_handle* h, double* f, const double* p, double thr_diag, double thr_non_diag,
                            double fp32_cutoff) {
     if (!h || !f || !p) return set_err(HFGPU_ERR_ARG, "null argument");

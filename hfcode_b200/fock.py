@@ -17,6 +17,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import threading
 from typing import Dict, Optional
 
 import numpy as np
@@ -39,6 +40,14 @@ REF_CLASSES = ["ss", "sp", "sd", "sl", "pp", "pd", "pl", "dd", "dl", "ll"]
 
 class HfgpuError(RuntimeError):
     pass
+
+
+# CUDA forbids device-synchronising calls (cudaFree, ...) in one thread while
+# another records a stream capture.  The library serialises its own captures
+# and allocations; callers that record their own graphs around library calls
+# (device_scf) hold this lock while recording, and handle creation, the
+# Schwarz pass (which sizes buffers) and release take it too.
+DEVICE_LOCK = threading.RLock()
 
 
 def _load():
@@ -70,6 +79,8 @@ def _load():
     lib.hfgpu_graph_capture.argtypes = [vp, vp, vp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
     lib.hfgpu_graph_launch.argtypes = [vp]
     lib.hfgpu_synchronize.argtypes = [vp]
+    lib.hfgpu_fock_build_device_on.argtypes = [vp, vp, vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, vp]
+    lib.hfgpu_small_solve.argtypes = [vp, vp, ctypes.c_int, vp, vp]
     lib.hfgpu_launch_count.argtypes = [vp, ll]
     lib.hfgpu_fock_build_graph.argtypes = [vp, d, d, ctypes.c_double, ctypes.c_double, ctypes.c_double]
     lib.hfgpu_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp)]
@@ -87,7 +98,8 @@ EXPORTS = ["hfgpu_init", "hfgpu_fock_build_initial_diag", "hfgpu_fock_build_diag
            "hfgpu_finalize", "hfgpu_last_error", "hfgpu_measure_fma_peak",
            "hfgpu_fock_build_diag_static", "hfgpu_one_electron", "hfgpu_set_scratch_budget",
            "hfgpu_device_bytes", "hfgpu_graph_capture", "hfgpu_graph_launch", "hfgpu_synchronize",
-           "hfgpu_fock_build_graph", "hfgpu_launch_count",
+           "hfgpu_fock_build_graph", "hfgpu_launch_count", "hfgpu_fock_build_device_on",
+           "hfgpu_small_solve",
            "hfgpu_batch_create", "hfgpu_batch_launch", "hfgpu_batch_destroy"]
 
 
@@ -121,14 +133,16 @@ class FockBuilder:
         self.nsh = shells.nsh
         self._desc = BasisDescriptor(shells)
         h = ctypes.c_void_p()
-        _check(_lib.hfgpu_init(ctypes.addressof(self._desc.struct), ctypes.byref(h)), "hfgpu_init")
+        with DEVICE_LOCK:
+            _check(_lib.hfgpu_init(ctypes.addressof(self._desc.struct), ctypes.byref(h)), "hfgpu_init")
         self.h = h
         if scratch_budget is not None:
             self.set_scratch_budget(scratch_budget)
 
     def close(self):
         if getattr(self, "h", None):
-            _lib.hfgpu_finalize(self.h)
+            with DEVICE_LOCK:
+                _lib.hfgpu_finalize(self.h)
             self.h = None
 
     def __del__(self):
@@ -148,7 +162,8 @@ class FockBuilder:
     # --- the reference's entry points -------------------------------------
     def fock_build_initial_diag(self, f: np.ndarray, p: np.ndarray, thr: float):
         fp, pp, keep = self._fp(f, p)
-        _check(_lib.hfgpu_fock_build_initial_diag(self.h, fp, pp, float(thr)), "fock_build_initial_diag")
+        with DEVICE_LOCK:
+            _check(_lib.hfgpu_fock_build_initial_diag(self.h, fp, pp, float(thr)), "fock_build_initial_diag")
 
     def fock_build_diag(self, f: np.ndarray, p: np.ndarray, thr: float):
         fp, pp, keep = self._fp(f, p)
@@ -195,6 +210,14 @@ class FockBuilder:
         fp, pp, keep = self._fp(f, p)
         _check(_lib.hfgpu_fock_build_graph(self.h, fp, pp, float(thr_diag), float(thr_non_diag),
                                            float(fp32_cutoff)), "fock_build_graph")
+
+    def fock_build_device_on(self, f_ptr: int, p_ptr: int, thr_diag: float, thr_non_diag: float,
+                             fp32_cutoff: float, stream: int):
+        """fock_build_device enqueued on `stream` with no host round trip
+        (safe inside the caller's CUDA-graph capture)."""
+        _check(_lib.hfgpu_fock_build_device_on(self.h, ctypes.c_void_p(f_ptr), ctypes.c_void_p(p_ptr),
+                                               float(thr_diag), float(thr_non_diag), float(fp32_cutoff),
+                                               ctypes.c_void_p(stream)), "fock_build_device_on")
 
     def graph_launch(self):
         """Enqueues one replay of the captured build on the handle's stream."""
@@ -262,3 +285,9 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def small_solve(a_ptr: int, b_ptr: int, n: int, status_ptr: int, stream: int):
+    """Device solve of A x = b (n <= 32, A row-major, x into b) on `stream`."""
+    _check(_lib.hfgpu_small_solve(ctypes.c_void_p(a_ptr), ctypes.c_void_p(b_ptr), int(n),
+                                  ctypes.c_void_p(status_ptr), ctypes.c_void_p(stream)), "small_solve")

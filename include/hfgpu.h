@@ -105,6 +105,20 @@ int hfgpu_synchronize(hfgpu_handle* h);
 int hfgpu_fock_build_graph(hfgpu_handle* h, double* f, const double* p, double thr_diag, double thr_non_diag,
                            double fp32_cutoff);
 
+/* One device build (as hfgpu_fock_build_device) enqueued on the caller's
+ * CUDA stream without any host round trip: launches are sized by the class
+ * capacities and the kernels read the survivor counts on the device, so a
+ * caller may record it inside its own stream capture (a whole device-resident
+ * SCF iteration as one graph).  No counterpart in the reference. */
+int hfgpu_fock_build_device_on(hfgpu_handle* h, double* f_dev, const double* p_dev, double thr_diag,
+                               double thr_non_diag, double fp32_cutoff, void* stream);
+
+/* Solves the small dense system A x = b (n <= 32; A row-major, overwritten;
+ * x replaces b) on the device, enqueued on `stream`: the DIIS equations of a
+ * device-resident SCF step (the role of wrapper_dsysv, wrapper_dsygv.f90:55-78).
+ * *status_dev (if not NULL) is set to 1, or 0 for a singular matrix. */
+int hfgpu_small_solve(double* a_dev, double* b_dev, int n, int* status_dev, void* stream);
+
 /* Several SCF instances' captured builds as one graph launch: one child
  * graph per handle, no dependencies between them, so independent molecules
  * fill the GPU together.  Every handle must hold a capture (and appear
