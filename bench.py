@@ -160,7 +160,7 @@ def mixed_study(fock, mol, sh, cutoffs, dev):
     from hfcode_b200 import basis, onee, scf
     bas = basis.load_basis("6-31G(d)")
     p0 = basis.density_superposition(mol, bas, sh.nb)
-    ints = onee.one_electron(mol, sh)
+    ints = onee.one_electron(mol, sh, gpu=True)
     out = {"cutoffs": {}}
     fb = fock.FockBuilder(sh)
     t0 = time.perf_counter()

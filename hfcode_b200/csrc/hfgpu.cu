@@ -63,6 +63,15 @@ thread_local std::string g_err;
 // library take this lock.
 std::recursive_mutex g_dev_mu;
 #define HF_DEVICE_LOCK std::lock_guard<std::recursive_mutex> dev_lock_(g_dev_mu)
+}  // namespace
+
+namespace hfgpu {
+// error text for entry points in other translation units (onee.cu)
+void set_last_error(const std::string& msg) { g_err = msg; }
+std::recursive_mutex& device_mutex() { return g_dev_mu; }
+}  // namespace hfgpu
+
+namespace {
 
 #define HF_CHECK(call)                                                                   \
     do {                                                                                 \

@@ -55,7 +55,7 @@ class DeviceSCF:
         self.sp2_steps = sp2_steps
         self.graphs = graphs
         self.dev = torch.device(device)
-        S, T, V = ints if ints is not None else onee.one_electron(mol, sh)
+        S, T, V = ints if ints is not None else onee.one_electron(mol, sh, gpu=True)
         e, U = np.linalg.eigh(S)
         X = (U / np.sqrt(e)) @ U.T  # S^-1/2 (direct_hartreefock.f90:22-29), once per job
         t = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device=self.dev)

@@ -99,7 +99,7 @@ EXPORTS = ["hfgpu_init", "hfgpu_fock_build_initial_diag", "hfgpu_fock_build_diag
            "hfgpu_fock_build_diag_static", "hfgpu_one_electron", "hfgpu_set_scratch_budget",
            "hfgpu_device_bytes", "hfgpu_graph_capture", "hfgpu_graph_launch", "hfgpu_synchronize",
            "hfgpu_fock_build_graph", "hfgpu_launch_count", "hfgpu_fock_build_device_on",
-           "hfgpu_small_solve",
+           "hfgpu_small_solve", "hfgpu_one_electron_gpu",
            "hfgpu_batch_create", "hfgpu_batch_launch", "hfgpu_batch_destroy"]
 
 

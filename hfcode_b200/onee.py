@@ -16,20 +16,28 @@ from .cabi import BasisDescriptor
 from . import fock
 
 
-def one_electron(mol: Molecule, sh: ShellSet):
+def one_electron(mol: Molecule, sh: ShellSet, gpu: bool = False):
+    """S, T, V over the shells: on the host (hfgpu_one_electron) or, with
+    gpu=True, on the current GPU (hfgpu_one_electron_gpu)."""
     lib = fock.lib()
     d = ctypes.POINTER(ctypes.c_double)
-    lib.hfgpu_one_electron.argtypes = [ctypes.c_void_p, ctypes.c_int, d, d, d, d, d]
+    fn = lib.hfgpu_one_electron_gpu if gpu else lib.hfgpu_one_electron
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_int, d, d, d, d, d]
     desc = BasisDescriptor(sh)
     nb = sh.nb
     S, T, V = (np.zeros((nb, nb)) for _ in range(3))
     z = np.ascontiguousarray(mol.charges, dtype=np.float64)
     x = np.ascontiguousarray(mol.coords, dtype=np.float64)
-    rc = lib.hfgpu_one_electron(ctypes.addressof(desc.struct), mol.natom, z.ctypes.data_as(d),
-                                x.ctypes.data_as(d), S.ctypes.data_as(d), T.ctypes.data_as(d),
-                                V.ctypes.data_as(d))
+    args = (ctypes.addressof(desc.struct), mol.natom, z.ctypes.data_as(d), x.ctypes.data_as(d),
+            S.ctypes.data_as(d), T.ctypes.data_as(d), V.ctypes.data_as(d))
+    if gpu:
+        with fock.DEVICE_LOCK:  # it allocates: not while another thread records a graph
+            rc = fn(*args)
+    else:
+        rc = fn(*args)
     if rc != 0:
-        raise fock.HfgpuError(f"hfgpu_one_electron failed ({rc})")
+        msg = lib.hfgpu_last_error().decode(errors="replace") if gpu else ""
+        raise fock.HfgpuError(f"{fn.__name__} failed ({rc}) {msg}")
     return S, T, V
 
 

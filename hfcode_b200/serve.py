@@ -155,7 +155,7 @@ class Server:
                 def __getattr__(s, name):
                     return getattr(s.inner, name)
 
-            ints = onee.one_electron(job.mol, job.sh)
+            ints = onee.one_electron(job.mol, job.sh, gpu=True)
             r = scf.direct_hartreefock(job.mol, job.sh, Tracked(fb), p_guess=job.p0, conve=self.conve,
                                        conv=self.conv, maxiter=60, ints=ints, fp32_cutoff=self.fp32_cutoff,
                                        graph=self.graphs)

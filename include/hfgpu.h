@@ -183,6 +183,12 @@ int hfgpu_measure_fma_peak(double* fp64_gflops, double* fp32_gflops);
 int hfgpu_one_electron(const hfgpu_basis* basis, int natom, const double* charges, const double* xyz,
                        double* S, double* T, double* V);
 
+/* The same S, T, V computed on the current GPU (one thread per shell pair,
+ * Obara-Saika recursions; host arrays in and out, temporary device buffers):
+ * the GPU version of cmpt1e.f90 / one_electron_terms.f90:7-1059. */
+int hfgpu_one_electron_gpu(const hfgpu_basis* basis, int natom, const double* charges, const double* xyz,
+                           double* S, double* T, double* V);
+
 /* fock_build_diag on device pointers for callers that cannot allocate GPU
  * memory at the call site -- for example code that runs where cudaMalloc is
  * not allowed, or that must not grow the device footprint after start-up.

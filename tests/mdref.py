@@ -163,3 +163,66 @@ def shell_eri(sh, s1, s2, s3, s4, boysfn=boys_exact, negab=True):
         if t == SHELL_D:
             acc = np.moveaxis(np.tensordot(HARM, np.moveaxis(acc, ax, 0), axes=(1, 0)), 0, ax)
     return acc.reshape(-1)
+
+
+def _prim_onee(la, lb, a, b, A, B, atoms):
+    """Primitive Cartesian overlap, kinetic and nuclear attraction by the
+    Hermite expansion (McMurchie-Davidson); atoms = [(Z, C), ...]."""
+    p = a + b
+    P = (a * A + b * B) / p
+
+    def s1(i, j, x):
+        return _E(i, j, 0, A[x] - B[x], a, b) * math.sqrt(math.pi / p) if i >= 0 and j >= 0 else 0.0
+
+    S = s1(la[0], lb[0], 0) * s1(la[1], lb[1], 1) * s1(la[2], lb[2], 2)
+    T = 0.0
+    for x in range(3):
+        o = [s1(la[y], lb[y], y) for y in range(3) if y != x]
+        l = lb[x]
+        d2 = l * (l - 1) * s1(la[x], l - 2, x) - 2 * b * (2 * l + 1) * s1(la[x], l, x) \
+            + 4 * b * b * s1(la[x], l + 2, x)
+        T += -0.5 * d2 * o[0] * o[1]
+    V = 0.0
+    L = sum(la) + sum(lb)
+    for Z, C in atoms:
+        PC = P - C
+        F = boys_exact(L, p * float(PC @ PC))
+        cache = {}
+        acc = 0.0
+        for t in range(la[0] + lb[0] + 1):
+            for u in range(la[1] + lb[1] + 1):
+                for v in range(la[2] + lb[2] + 1):
+                    acc += _E(la[0], lb[0], t, A[0] - B[0], a, b) * _E(la[1], lb[1], u, A[1] - B[1], a, b) * \
+                        _E(la[2], lb[2], v, A[2] - B[2], a, b) * _R(t, u, v, 0, p, PC[0], PC[1], PC[2], F, cache)
+        V += -Z * 2 * math.pi / p * acc
+    return S, T, V
+
+
+def shell_onee(sh, s1, s2, atoms):
+    """Contracted (S, T, V) blocks of shells s1, s2 (functions in the
+    reference's order, spherical d), with the L-shell p/s ratio."""
+    typ = [int(sh.shtyp[s1]), int(sh.shtyp[s2])]
+    X = [np.asarray(sh.xsh[s], dtype=float) for s in (s1, s2)]
+    carts = [CART[t] for t in typ]
+    out = [np.zeros((len(carts[0]), len(carts[1]))) for _ in range(3)]
+    for za in range(sh.nzet[s1]):
+        for zb in range(sh.nzet[s2]):
+            ea, eb = sh.zeta[s1, za], sh.zeta[s2, zb]
+            for i, ca in enumerate(carts[0]):
+                for j, cb in enumerate(carts[1]):
+                    w = sh.djk[s1, za] * sh.djk[s2, zb]
+                    if typ[0] == SHELL_L and sum(ca) == 1:
+                        w *= sh.djkl[s1, za]
+                    if typ[1] == SHELL_L and sum(cb) == 1:
+                        w *= sh.djkl[s2, zb]
+                    vals = _prim_onee(ca, cb, ea, eb, X[0], X[1], atoms)
+                    for k in range(3):
+                        out[k][i, j] += w * vals[k]
+    res = []
+    for blk in out:
+        if typ[0] == SHELL_D:
+            blk = HARM @ blk
+        if typ[1] == SHELL_D:
+            blk = blk @ HARM.T
+        res.append(blk)
+    return res
