@@ -585,6 +585,8 @@ def class_params(tag: str) -> dict:
     if os.path.exists(_TUNING_FILE):
         with open(_TUNING_FILE) as fh:
             prm.update(json.load(fh).get(tag, {}))
+    prm.setdefault("acc_max32", 2 * prm["acc_max"])
+    prm.setdefault("out_max32", 2 * prm["out_max"])
     return prm
 
 
@@ -648,35 +650,46 @@ def class_source(ci: int, bi: int, ki: int):
         info.update(roles=1, role_sizes=[g.nout], role_outs=[roles[0]], acc_groups=[])
     elif len(roles) <= prm["max_roles2"]:
         mode = "staged2"
-        for r, outs in enumerate(roles):
-            code, _ = g.emit_role(f"{g.name}_r{r}", outs)
-            code32, _ = g32.emit_role(f"{g32.name}_r{r}", outs)
-            funcs += [code, code32]
-            stores = "\n".join(f"    {{ const double v = (double)e[{i}]; out[(size_t){n} * a.stride + t] = (Real)v; "
+        # FP32 values take half the registers: the FP32 kernels use roles of
+        # twice the size, so fewer of them repeat the primitive loop
+        roles32 = g.partition(prm["acc_max32"], prm["out_max32"])
+
+        def s2_kernel(kname, fname, outs, r, f32):
+            real = "float" if f32 else "double"
+            stores = "\n".join(f"    {{ const double v = (double)e[{i}]; out[(size_t){n} * a.stride + t] = ({real})v; "
                                f"mx = fmax(mx, fabs(v)); }}" for i, n in enumerate(outs))
-            kern.append(f"""
-template <bool F32>
-__global__ void __launch_bounds__(ND_THREADS, F32 ? 3 : 2) k_s2_{g.tag}_r{r}(StagedArgs a) {{
-    using Real = typename std::conditional<F32, float, double>::type;
-    __shared__ Real sboys[BOYS_NPT * BOYS_K];
-    if constexpr (F32) stage_boys<{g.L}>(sboys, a.boysf);
-    else stage_boys<{g.L}>(sboys, a.boys);
+            tab = "a.boysf" if f32 else "a.boys"
+            return f"""
+__global__ void __launch_bounds__(ND_THREADS, {3 if f32 else 2}) {kname}(StagedArgs a) {{
+    __shared__ {real} sboys[BOYS_NPT * BOYS_K];
+    stage_boys<{g.L}>(sboys, {tab});
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= staged_count(a)) return;
     const uint2 q = staged_quartet(a, t);
     const GPair bra = a.bra[q.x];
     const GPair ket = a.ket[q.y];
-    Real e[{len(outs)}];
-    if constexpr (F32) eri_{g.tag}_f32_r{r}(bra, ket, a.prims, sboys, e);
-    else eri_{g.tag}_r{r}(bra, ket, a.prims, sboys, e);
+    {real} e[{len(outs)}];
+    {fname}(bra, ket, a.prims, sboys, e);
     double mx = 0.0;
-    Real* out = reinterpret_cast<Real*>(a.out);  // FP32 chunks keep FP32 rows
+    {real}* out = reinterpret_cast<{real}*>(a.out);  // FP32 chunks keep FP32 rows
 {stores}
     a.mx[(size_t){r} * a.stride + t] = mx;
-}}""")
-        reg.append(f"    k->mode = 1;\n    k->nacc = 0;\n    k->nrole_a = 0;\n    k->nrole_b = {len(roles)};")
+}}"""
+
+        for r, outs in enumerate(roles):
+            code, _ = g.emit_role(f"{g.name}_r{r}", outs)
+            funcs.append(code)
+            kern.append(s2_kernel(f"k_s2_{g.tag}_r{r}", f"eri_{g.tag}_r{r}", outs, r, False))
+        for r, outs in enumerate(roles32):
+            code32, _ = g32.emit_role(f"{g32.name}_r{r}", outs)
+            funcs.append(code32)
+            kern.append(s2_kernel(f"k_s2f_{g.tag}_r{r}", f"eri_{g.tag}_f32_r{r}", outs, r, True))
+        reg.append(f"    k->mode = 1;\n    k->nacc = 0;\n    k->nrole_a = 0;\n    k->nrole_b = {len(roles)};\n"
+                   f"    k->nrole_b32 = {len(roles32)};")
         for r in range(len(roles)):
-            reg.append(f"    k->sb64[{r}] = k_s2_{g.tag}_r{r}<false>;\n    k->sb32[{r}] = k_s2_{g.tag}_r{r}<true>;")
+            reg.append(f"    k->sb64[{r}] = k_s2_{g.tag}_r{r};")
+        for r in range(len(roles32)):
+            reg.append(f"    k->sb32[{r}] = k_s2f_{g.tag}_r{r};")
         reg.append(f"    k->scat = k_scatter_staged<{NA}, {NB}, {NC}, {ND}>;\n"
                    f"    k->scat_smem = scat_smem_bytes({NA}, {NB}, {NC}, {ND});\n"
                    f"    k->scat32 = k_scatter_staged<{NA}, {NB}, {NC}, {ND}, float>;\n"
@@ -684,6 +697,7 @@ __global__ void __launch_bounds__(ND_THREADS, F32 ? 3 : 2) k_s2_{g.tag}_r{r}(Sta
         if bi == ki:
             reg.append(f"    k->diag0 = nullptr;\n    k->diag1 = nullptr;")
             reg.append(f"    k->dscat0 = k_scatter_diag<{NA}, {NB}, 0>;\n    k->dscat1 = k_scatter_diag<{NA}, {NB}, 1>;")
+        info["role_outs32"] = roles32
         info.update(roles=len(roles), role_sizes=[len(x) for x in roles], role_outs=roles, acc_groups=[])
     else:
         mode = "staged3"
@@ -729,7 +743,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_sb_{g.tag}_r{r}(StagedArgs a) {{
         hrr_{g.tag}_r{r}(bra, ket, a.acc + t, a.out + (size_t){outs[0]} * a.stride + t, a.stride);
 }}""")
         reg.append(f"    k->mode = 2;\n    k->nacc = {len(keyidx)};\n    k->nrole_a = {len(groups)};\n"
-                   f"    k->nrole_b = {len(outroles)};")
+                   f"    k->nrole_b = {len(outroles)};\n    k->nrole_b32 = {len(outroles)};")
         for r in range(len(groups)):
             reg.append(f"    k->sa64[{r}] = k_sa_{g.tag}_r{r}<false>;\n    k->sa32[{r}] = k_sa_{g.tag}_r{r}<true>;")
         for r in range(len(outroles)):
@@ -875,10 +889,15 @@ def main(outdir: str):
             for r, outs in enumerate(info["role_outs"]):
                 n = len(outs)
                 idx = ", ".join(map(str, outs))
-                lines.append(f"    {{ static const int ix[{n}] = {{{idx}}}; double o[{n}]; float of[{n}];")
-                lines.append(f"      if (f32) {{ eri_{tag}_f32_r{r}(b, k, p, tf, of); for (int i = 0; i < {n}; ++i) o[i] = of[i]; }}")
-                lines.append(f"      else eri_{tag}_r{r}(b, k, p, t, o);")
+                lines.append(f"    if (!f32) {{ static const int ix[{n}] = {{{idx}}}; double o[{n}];")
+                lines.append(f"      eri_{tag}_r{r}(b, k, p, t, o);")
                 lines.append(f"      for (int i = 0; i < {n}; ++i) out[ix[i]] = o[i]; }}")
+            for r, outs in enumerate(info["role_outs32"]):
+                n = len(outs)
+                idx = ", ".join(map(str, outs))
+                lines.append(f"    if (f32) {{ static const int ix[{n}] = {{{idx}}}; float of[{n}];")
+                lines.append(f"      eri_{tag}_f32_r{r}(b, k, p, tf, of);")
+                lines.append(f"      for (int i = 0; i < {n}; ++i) out[ix[i]] = of[i]; }}")
         else:
             nacc = sum(len(g) for g in info["acc_groups"])
             lines.append(f"    static double acc[{nacc}];")

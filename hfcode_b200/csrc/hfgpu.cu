@@ -684,7 +684,7 @@ int build_active(hfgpu_handle* h) {
         const ClassKernels& K = CLASS_KERNELS[c];
         h->stride[c] = 0;
         if (K.mode == 0 || h->ccap[c] == 0) continue;
-        const size_t per = (size_t)K.nacc + K.nout + K.nrole_b;
+        const size_t per = (size_t)K.nacc + K.nout + std::max(K.nrole_b, K.nrole_b32);
         size_t st = std::min<size_t>((size_t)h->ccap[c], budget / per);
         st = std::max<size_t>(st, 128);
         h->stride[c] = st;
@@ -727,7 +727,7 @@ int run_staged(hfgpu_handle* h, int c, int prec, long long n, const double* P, d
         a.out = scratch + (size_t)K.nacc * st;
         a.mx = scratch + (size_t)(K.nacc + K.nout) * st;
         a.stride = st;
-        a.nroles = K.nrole_b;
+        a.nroles = prec ? K.nrole_b32 : K.nrole_b;
         a.P = P;
         a.G = h->d_G;
         a.nb = h->nb;
@@ -741,7 +741,7 @@ int run_staged(hfgpu_handle* h, int c, int prec, long long n, const double* P, d
             (prec ? K.sa32[r] : K.sa64[r])<<<blocks, ND_THREADS, 0, stream>>>(a);
             HF_CHECK(cudaGetLastError());
         }
-        for (int r = 0; r < K.nrole_b; ++r) {
+        for (int r = 0; r < a.nroles; ++r) {
             ++h->launches;
             (prec ? K.sb32[r] : K.sb64[r])<<<blocks, ND_THREADS, 0, stream>>>(a);
             HF_CHECK(cudaGetLastError());
