@@ -660,7 +660,7 @@ def class_source(ci: int, bi: int, ki: int):
                                f"mx = fmax(mx, fabs(v)); }}" for i, n in enumerate(outs))
             tab = "a.boysf" if f32 else "a.boys"
             return f"""
-__global__ void __launch_bounds__(ND_THREADS, {3 if f32 else 2}) {kname}(StagedArgs a) {{
+__global__ void __launch_bounds__(ND_THREADS, 2) {kname}(StagedArgs a) {{
     __shared__ {real} sboys[BOYS_NPT * BOYS_K];
     stage_boys<{g.L}>(sboys, {tab});
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
