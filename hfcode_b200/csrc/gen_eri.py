@@ -661,8 +661,10 @@ def class_source(ci: int, bi: int, ki: int):
             tab = "a.boysf" if f32 else "a.boys"
             return f"""
 __global__ void __launch_bounds__(ND_THREADS, 2) {kname}(StagedArgs a) {{
-    __shared__ {real} sboys[BOYS_NPT * BOYS_K];
-    stage_boys<{g.L}>(sboys, {tab});
+    // Boys table of order L read through the L1 cache: with a few primitive
+    // quartets per shell quartet, staging it in shared memory per block
+    // costs more than the lookups it serves
+    const {real}* __restrict__ sboys = {tab} + (size_t){g.L} * BOYS_NPT * BOYS_K;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= staged_count(a)) return;
     const uint2 q = staged_quartet(a, t);
@@ -715,9 +717,9 @@ __global__ void __launch_bounds__(ND_THREADS, 2) {kname}(StagedArgs a) {{
 template <bool F32>
 __global__ void __launch_bounds__(ND_THREADS, F32 ? 3 : 2) k_sa_{g.tag}_r{r}(StagedArgs a) {{
     using Real = typename std::conditional<F32, float, double>::type;
-    __shared__ Real sboys[BOYS_NPT * BOYS_K];
-    if constexpr (F32) stage_boys<{g.L}>(sboys, a.boysf);
-    else stage_boys<{g.L}>(sboys, a.boys);
+    const Real* __restrict__ sboys;  // Boys table of order L, through the L1 cache
+    if constexpr (F32) sboys = a.boysf + (size_t){g.L} * BOYS_NPT * BOYS_K;
+    else sboys = a.boys + (size_t){g.L} * BOYS_NPT * BOYS_K;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= staged_count(a)) return;
     const uint2 q = staged_quartet(a, t);
