@@ -321,7 +321,7 @@ class ClassGen:
         w(f"        const {ft} p = {cv('pb.p')};")
         w(f"        const {ft} PA0 = {cv('pb.P[0] - Ax')}, PA1 = {cv('pb.P[1] - Ay')}, PA2 = {cv('pb.P[2] - Az')};")
         if L > 0:
-            w(f"        const {ft} h2p1 = {'0.5' if dbl else '0.5f'} / p;  // bra-only, out of the ket loop")
+            w(f"        const {ft} h2p1 = {cv('pb.pad')};  // 1/(2p), precomputed per primitive pair")
         used_b = sorted({k[0] for k in acc})
         used_k = sorted({k[1] for k in acc})
         for bi in used_b:
@@ -362,7 +362,7 @@ class ClassGen:
                 w("            const float QC0 = (float)(pk.P[0] - Cx), QC1 = (float)(pk.P[1] - Cy), "
                   "QC2 = (float)(pk.P[2] - Cz);")
             w(f"            const {ft} rp = qo, rq = po;  // rho/p = q/(p+q), rho/q = p/(p+q)")
-            w(f"            const {ft} h2q1 = {half} / q;")
+            w(f"            const {ft} h2q1 = {cv('pk.pad')};  // 1/(2q), precomputed per primitive pair")
             w(f"            const {ft} h2pq1 = {half} * opq;")
             for n in range(2, 5):
                 w(f"            const {ft} h2p{n} = {n} * h2p1, h2q{n} = {n} * h2q1, h2pq{n} = {n} * h2pq1;")

@@ -933,7 +933,7 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
     const size_t nb2 = (size_t)h->nb * h->nb;
     rc |= dalloc(&h->d_shtyp, h->nsh);
     rc |= dalloc(&h->d_aosh, h->nsh);
-    rc |= dalloc(&h->d_psoa, 7 * std::max<size_t>(prims.size(), 1));
+    rc |= dalloc(&h->d_psoa, 8 * std::max<size_t>(prims.size(), 1));
     rc |= dalloc(&h->d_boys, bt.size());
     rc |= dalloc(&h->d_boysf, btf.size());
     rc |= dalloc(&h->d_P, nb2);
@@ -1306,12 +1306,12 @@ int hfgpu_device_bytes(const hfgpu_handle* h, size_t* bytes) {
     b += 3 * nb2 * sizeof(double);                            // P, F, G
     b += (size_t)h->nsh * h->nsh * sizeof(double);            // maxdm
     b += 2 * (size_t)h->nsh * sizeof(int);
-    b += 7 * h->hprims.size() * sizeof(double);               // all-pairs primitives
+    b += 8 * h->hprims.size() * sizeof(double);               // all-pairs primitives
     for (int t = 0; t < NPT; ++t) {
         const size_t n = h->pairs[t].size();
         b += n * (2 * sizeof(GPair) + sizeof(double) * 2 + sizeof(int2) + (h->d_diaglist[t] ? sizeof(uint2) : 0));
     }
-    b += 7 * h->naprims * sizeof(double);                     // active-list primitives
+    b += 8 * h->naprims * sizeof(double);                     // active-list primitives
     b += h->qcap * sizeof(uint2);                             // quartet lists
     b += h->scratch_doubles * sizeof(double);                 // staged scratch
     b += h->subcap * (sizeof(ScreenSub) + 2 * sizeof(unsigned long long));

@@ -49,6 +49,7 @@ struct PrimSoA {
     const double* K;
     const double* w1;
     const double* w2;
+    const double* h;   // 1/(2p), precomputed on the host
 };
 
 __device__ __forceinline__ GPrim load_prim(const PrimSoA& s, int i) {
@@ -60,7 +61,7 @@ __device__ __forceinline__ GPrim load_prim(const PrimSoA& s, int i) {
     g.K = __ldg(s.K + i);
     g.w1 = __ldg(s.w1 + i);
     g.w2 = __ldg(s.w2 + i);
-    g.pad = 0.0;
+    g.pad = __ldg(s.h + i);  // 1/(2p)
     return g;
 }
 
