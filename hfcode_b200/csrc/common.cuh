@@ -183,8 +183,8 @@ struct NDArgs {
 
 template <int M, typename T>
 __device__ __forceinline__ void stage_boys(T* sm, const T* g) {
-    const T* src = g + (size_t)M * BOYS_NPT * BOYS_K;
-    for (int i = threadIdx.x; i < BOYS_NPT * BOYS_K; i += blockDim.x) sm[i] = src[i];
+    const T* src = g + (size_t)M * BOYS_BLK;
+    for (int i = threadIdx.x; i < BOYS_BLK; i += blockDim.x) sm[i] = src[i];
     __syncthreads();
 }
 
@@ -208,7 +208,7 @@ constexpr int ND_THREADS = 128;
 template <class C, bool F32>
 __global__ void __launch_bounds__(ND_THREADS) k_nondiag(NDArgs a) {
     using Real = typename std::conditional<F32, float, double>::type;
-    __shared__ Real sboys[BOYS_NPT * BOYS_K];
+    __shared__ Real sboys[BOYS_BLK];
     if constexpr (F32) stage_boys<C::LL>(sboys, a.boysf);
     else stage_boys<C::LL>(sboys, a.boys);
     constexpr int NA = pt_na(C::BI), NB = pt_nb(C::BI), NC = pt_na(C::KI), ND = pt_nb(C::KI);
@@ -263,7 +263,7 @@ struct DiagArgs {
 // and fock_build_diag.f90 (MODE 1).
 template <class C, int MODE>
 __global__ void __launch_bounds__(ND_THREADS) k_diag(DiagArgs a) {
-    __shared__ double sboys[BOYS_NPT * BOYS_K];
+    __shared__ double sboys[BOYS_BLK];
     stage_boys<C::LL>(sboys, a.boys);
     constexpr int NA = pt_na(C::BI), NB = pt_nb(C::BI);
     const int t = blockIdx.x * blockDim.x + threadIdx.x;

@@ -664,7 +664,7 @@ __global__ void __launch_bounds__(ND_THREADS, 2) {kname}(StagedArgs a) {{
     // Boys table of order L read through the L1 cache: with a few primitive
     // quartets per shell quartet, staging it in shared memory per block
     // costs more than the lookups it serves
-    const {real}* __restrict__ sboys = {tab} + (size_t){g.L} * BOYS_NPT * BOYS_K;
+    const {real}* __restrict__ sboys = {tab} + (size_t){g.L} * BOYS_BLK;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= staged_count(a)) return;
     const uint2 q = staged_quartet(a, t);
@@ -718,8 +718,8 @@ template <bool F32>
 __global__ void __launch_bounds__(ND_THREADS, F32 ? 3 : 2) k_sa_{g.tag}_r{r}(StagedArgs a) {{
     using Real = typename std::conditional<F32, float, double>::type;
     const Real* __restrict__ sboys;  // Boys table of order L, through the L1 cache
-    if constexpr (F32) sboys = a.boysf + (size_t){g.L} * BOYS_NPT * BOYS_K;
-    else sboys = a.boys + (size_t){g.L} * BOYS_NPT * BOYS_K;
+    if constexpr (F32) sboys = a.boysf + (size_t){g.L} * BOYS_BLK;
+    else sboys = a.boys + (size_t){g.L} * BOYS_BLK;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= staged_count(a)) return;
     const uint2 q = staged_quartet(a, t);
@@ -788,7 +788,7 @@ def role_kernels(g: "ClassGen", roles, diag: bool, diag_only: bool = False) -> s
     return f"""
 template <int MODE>
 __global__ void __launch_bounds__({32 * R}) k_dg_{tag}(DiagArgs a) {{
-    __shared__ double sboys[BOYS_NPT * BOYS_K];
+    __shared__ double sboys[BOYS_BLK];
     __shared__ double smax[{32 * R}];
     stage_boys<{L}>(sboys, a.boys);
     const int lane = threadIdx.x & 31, role = threadIdx.x >> 5;

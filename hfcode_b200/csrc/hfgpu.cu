@@ -1315,7 +1315,7 @@ int hfgpu_device_bytes(const hfgpu_handle* h, size_t* bytes) {
     b += h->qcap * sizeof(uint2);                             // quartet lists
     b += h->scratch_doubles * sizeof(double);                 // staged scratch
     b += h->subcap * (sizeof(ScreenSub) + 2 * sizeof(unsigned long long));
-    b += (size_t)(BOYS_MMAX + 1) * BOYS_NPT * BOYS_K * (sizeof(double) + sizeof(float));
+    b += (size_t)(BOYS_MMAX + 1) * BOYS_BLK * (sizeof(double) + sizeof(float));
     *bytes = b;
     return HFGPU_OK;
 }

@@ -118,9 +118,10 @@ inline long double boys_series(int m, long double T) {
     return expl(-T) * sum;
 }
 
-// Boys Taylor tables: c_k = F_{M+k}(T_j) (-1)^k / k!, M = 0..8, T_j = j/8.
+// Boys Taylor tables: c_k = F_{M+k}(T_j) (-1)^k / k!, M = 0..8, T_j = j/8;
+// each order's block ends with exp(-T_j) for the downward recursion.
 inline void build_boys_table(std::vector<double>& bt, std::vector<float>& btf) {
-    bt.assign((size_t)(BOYS_MMAX + 1) * BOYS_NPT * BOYS_K, 0.0);
+    bt.assign((size_t)(BOYS_MMAX + 1) * BOYS_BLK, 0.0);
     btf.assign(bt.size(), 0.0f);
     for (int M = 0; M <= BOYS_MMAX; ++M)
         for (int j = 0; j < BOYS_NPT; ++j) {
@@ -128,10 +129,13 @@ inline void build_boys_table(std::vector<double>& bt, std::vector<float>& btf) {
             for (int k = 0; k < BOYS_K; ++k) {
                 if (k) fact *= k;
                 long double v = boys_series(M + k, T) / fact * ((k & 1) ? -1.0L : 1.0L);
-                size_t i = ((size_t)M * BOYS_NPT + j) * BOYS_K + k;
+                size_t i = (size_t)M * BOYS_BLK + (size_t)j * BOYS_K + k;
                 bt[i] = (double)v;
                 btf[i] = (float)v;
             }
+            const size_t ie = (size_t)M * BOYS_BLK + (size_t)BOYS_NPT * BOYS_K + j;
+            bt[ie] = (double)expl(-T);
+            btf[ie] = (float)expl(-T);
         }
 }
 

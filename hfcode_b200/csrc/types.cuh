@@ -13,6 +13,9 @@ constexpr int NPT = 10;                 // GPU pair types SS LS LL DS DL DD PS L
 constexpr int NCLS = 55;                // quartet classes over the pair types (21 without pure p)
 constexpr int BOYS_NPT = 225;           // grid T_j = j/8, j = 0..224 (T <= 28)
 constexpr int BOYS_K = 8;               // Taylor terms per grid point
+// one block per order M: BOYS_NPT x BOYS_K Taylor coefficients, then the
+// BOYS_NPT values exp(-T_j) used by the downward recursion
+constexpr int BOYS_BLK = BOYS_NPT * (BOYS_K + 1);
 constexpr int BOYS_MMAX = 8;            // highest order used: (dd|dd)
 
 // Primitive pair (one surviving primitive product of a shell pair): exponent
@@ -75,8 +78,9 @@ __device__ __forceinline__ GPrim load_prim(const PrimSoA& s, int i) {
 template <int M>
 __device__ __forceinline__ void boys_eval(double T, const double* __restrict__ tab, double* F) {
     if (T > 28.0) {
-        const double it = 1.0 / T;
-        F[0] = 0.88622692545275801365 * sqrt(it);
+        const double rt = rsqrt(T);  // one reciprocal square root gives sqrt(1/T) and 1/T
+        const double it = rt * rt;
+        F[0] = 0.88622692545275801365 * rt;
 #pragma unroll
         for (int m = 1; m <= M; ++m) F[m] = F[m - 1] * ((m - 0.5) * it);
     } else {
@@ -88,7 +92,20 @@ __device__ __forceinline__ void boys_eval(double T, const double* __restrict__ t
         for (int k = BOYS_K - 2; k >= 0; --k) f = fma(f, x, c[k]);
         F[M] = f;
         if (M > 0) {
-            const double e = exp(-T);
+            // exp(-T) = exp(-T_j) exp(-x), |x| <= 1/16: ten Taylor terms of
+            // exp(-x) leave a truncation error below 3e-19
+            double ex = 1.0 / 3628800.0;
+            ex = fma(ex, -x, 1.0 / 362880.0);
+            ex = fma(ex, -x, 1.0 / 40320.0);
+            ex = fma(ex, -x, 1.0 / 5040.0);
+            ex = fma(ex, -x, 1.0 / 720.0);
+            ex = fma(ex, -x, 1.0 / 120.0);
+            ex = fma(ex, -x, 1.0 / 24.0);
+            ex = fma(ex, -x, 1.0 / 6.0);
+            ex = fma(ex, -x, 0.5);
+            ex = fma(ex, -x, 1.0);
+            ex = fma(ex, -x, 1.0);
+            const double e = tab[BOYS_NPT * BOYS_K + j] * ex;
             const double t2 = T + T;
 #pragma unroll
             for (int m = M - 1; m >= 0; --m) F[m] = fma(t2, F[m + 1], e) * (1.0 / (2 * m + 1));
@@ -99,8 +116,9 @@ __device__ __forceinline__ void boys_eval(double T, const double* __restrict__ t
 template <int M>
 __device__ __forceinline__ void boys_eval(float T, const float* __restrict__ tab, float* F) {
     if (T > 28.0f) {
-        const float it = 1.0f / T;
-        F[0] = 0.886226925f * sqrtf(it);
+        const float rt = rsqrtf(T);
+        const float it = rt * rt;
+        F[0] = 0.886226925f * rt;
 #pragma unroll
         for (int m = 1; m <= M; ++m) F[m] = F[m - 1] * ((m - 0.5f) * it);
     } else {

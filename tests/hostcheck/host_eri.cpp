@@ -37,7 +37,29 @@ struct HC {
     std::vector<float> btf;
 };
 
+template <int M>
+static void boys_m(const double* bt, double T, double* out) {
+    boys_eval<M>(T, bt + (size_t)M * BOYS_BLK, out);
+}
+
 extern "C" {
+
+// F_0..F_M(T) from the device Boys evaluation (table, Taylor, downward
+// recursion with the tabulated exponential), compiled for the host
+void hc_boys(const void* hv, int M, double T, double* out) {
+    const double* bt = ((const HC*)hv)->bt.data();
+    switch (M) {
+        case 0: boys_m<0>(bt, T, out); break;
+        case 1: boys_m<1>(bt, T, out); break;
+        case 2: boys_m<2>(bt, T, out); break;
+        case 3: boys_m<3>(bt, T, out); break;
+        case 4: boys_m<4>(bt, T, out); break;
+        case 5: boys_m<5>(bt, T, out); break;
+        case 6: boys_m<6>(bt, T, out); break;
+        case 7: boys_m<7>(bt, T, out); break;
+        default: boys_m<8>(bt, T, out); break;
+    }
+}
 
 void* hc_create(const hfgpu_basis* B) {
     HC* h = new HC();
@@ -56,8 +78,8 @@ int hc_eri(void* hh, int cls, int L, int a, int b, int c, int d, int f32, double
     GPair ket = make_pair(h->B, c, d, prims);
     std::vector<double> soa = prims_soa(prims);
     const PrimSoA ps = soa_view(soa.data(), prims.size());
-    const double* t = h->bt.data() + (size_t)L * BOYS_NPT * BOYS_K;
-    const float* tf = h->btf.data() + (size_t)L * BOYS_NPT * BOYS_K;
+    const double* t = h->bt.data() + (size_t)L * BOYS_BLK;
+    const float* tf = h->btf.data() + (size_t)L * BOYS_BLK;
     HOST_ERI[cls](bra, ket, ps, t, tf, out, f32);
     return 0;
 }

@@ -60,6 +60,7 @@ def _build():
     lib.hc_eri.argtypes = [vp, i, i, i, i, i, i, i, d]
     lib.hc_scatter.argtypes = [vp, i, i, i, i, i, d, ctypes.c_double, d, d, i, i]
     lib.hc_scatter.restype = i
+    lib.hc_boys.argtypes = [vp, i, ctypes.c_double, d]
     return lib, json.load(open(os.path.join(GEN, "class_flops.json")))
 
 
@@ -144,3 +145,23 @@ def test_generated_scatter_matches_uniform_scatter(host):
                 assert np.max(np.abs(G - R)) < 1e-12 * max(1.0, np.max(np.abs(R))), (info[str(ci)]["name"], q)
                 checked += 1
     assert checked > 0
+
+
+def test_device_boys_matches_exact(host):
+    """The kernels' Boys function (8-term Taylor on a 1/8 grid, downward
+    recursion with exp(-T) from the table and a 10-term Taylor factor)
+    against mpmath below T = 28, and the reference's asymptotic form above."""
+    import mdref
+    lib, _ = host
+    _, _, sh, _ = system("water")
+    desc = BasisDescriptor(sh)
+    h = lib.hc_create(ctypes.addressof(desc.struct))
+    rng = np.random.default_rng(5)
+    Ts = np.concatenate([[0.0, 1e-9, 0.0625, 0.125, 7.9375, 27.99], rng.uniform(0, 28, 40), rng.uniform(28.01, 60, 8)])
+    for M in range(9):
+        for T in Ts:
+            out = np.zeros(9)
+            lib.hc_boys(h, M, float(T), _dp(out))
+            ref = mdref.boys_ref_longrange(M, float(T))
+            rel = np.max(np.abs(out[:M + 1] - ref) / np.abs(ref))
+            assert rel < 5e-14, (M, T, rel)
