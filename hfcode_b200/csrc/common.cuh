@@ -317,6 +317,8 @@ struct StagedArgs {
     int jonly;
     int f32;
     ClassStats* stats;
+    const double* Pb;      // density in shell-pair blocks (staged scatter)
+    const int* boff;       // block offsets, nsh x nsh
     // diagonal builders only
     double* schw;          // per pair (MODE 0 writes, MODE 1 reads)
     const double* md;      // nsh x nsh density maxima
@@ -377,13 +379,21 @@ __host__ __device__ constexpr int scat_smem_bytes(int NA, int NB, int NC, int ND
 // integrals are FP32 already; the sums go into G with FP64 atomics).
 template <int NA, int NB, int NC, int ND, typename E>
 __device__ __forceinline__ void scatter_async(const E* __restrict__ e, size_t st, double s, const GPair& bra,
-                                              const GPair& ket, const double* __restrict__ P,
+                                              const GPair& ket, const double* __restrict__ Pb,
+                                              const int* __restrict__ boff, int nsh,
                                               double* __restrict__ G, int nb, bool jonly, E* sm) {
     constexpr int T = ND_THREADS, SLAB = NC * ND, NS = NA * NB;
     constexpr int NBUF = scat_nbuf(NA, NB, NC, ND, (int)sizeof(E));
     const int tid = threadIdx.x;
     const int a0 = bra.aoa, b0 = bra.aob, c0 = ket.aoa, d0 = ket.aob;
-    auto Pm = [&](int r, int c) { return (E)__ldg(P + r + (size_t)c * nb); };
+    // density blocks in shell-pair order (row-major within a block), so each
+    // row a thread reads is contiguous instead of one access per column
+    const double* __restrict__ Bab = Pb + __ldg(boff + bra.sa * nsh + bra.sb);
+    const double* __restrict__ Bac = Pb + __ldg(boff + bra.sa * nsh + ket.sa);
+    const double* __restrict__ Bad = Pb + __ldg(boff + bra.sa * nsh + ket.sb);
+    const double* __restrict__ Bbc = Pb + __ldg(boff + bra.sb * nsh + ket.sa);
+    const double* __restrict__ Bbd = Pb + __ldg(boff + bra.sb * nsh + ket.sb);
+    const double* __restrict__ Bcd = Pb + __ldg(boff + ket.sa * nsh + ket.sb);
     auto Ga = [&](int r, int c) { return G + r + (size_t)c * nb; };
     E* eb = sm + tid;                      // [NBUF][SLAB][T], this thread's column
     E* pk = sm + NBUF * SLAB * T + tid;    // [NB*NC] P_bc then [NB*ND] P_bd
@@ -401,9 +411,9 @@ __device__ __forceinline__ void scatter_async(const E* __restrict__ e, size_t st
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
 #pragma unroll
-        for (int k = 0; k < NC; ++k) pk[(j * NC + k) * T] = Pm(b0 + j, c0 + k);
+        for (int k = 0; k < NC; ++k) pk[(j * NC + k) * T] = (E)__ldg(Bbc + j * NC + k);
 #pragma unroll
-        for (int l = 0; l < ND; ++l) pk[(NB * NC + j * ND + l) * T] = Pm(b0 + j, d0 + l);
+        for (int l = 0; l < ND; ++l) pk[(NB * NC + j * ND + l) * T] = (E)__ldg(Bbd + j * ND + l);
     }
     const E s2 = (E)(2.0 * s), hs = (E)(-0.5 * s);
     E jcd[NC * ND], kbc[NB * NC], kbd[NB * ND], pcd[NC * ND];
@@ -416,7 +426,7 @@ __device__ __forceinline__ void scatter_async(const E* __restrict__ e, size_t st
 #pragma unroll
     for (int k = 0; k < NC; ++k)
 #pragma unroll
-        for (int l = 0; l < ND; ++l) pcd[k * ND + l] = Pm(c0 + k, d0 + l);
+        for (int l = 0; l < ND; ++l) pcd[k * ND + l] = (E)__ldg(Bcd + k * ND + l);
 #pragma unroll 1
     for (int i = 0; i < NA; ++i) {
         E jab[NB], kac[NC], kad[ND], pad_[ND], pac[NC];
@@ -425,12 +435,12 @@ __device__ __forceinline__ void scatter_async(const E* __restrict__ e, size_t st
 #pragma unroll
         for (int k = 0; k < NC; ++k) {
             kac[k] = 0;
-            pac[k] = Pm(a0 + i, c0 + k);
+            pac[k] = (E)__ldg(Bac + i * NC + k);
         }
 #pragma unroll
         for (int l = 0; l < ND; ++l) {
             kad[l] = 0;
-            pad_[l] = Pm(a0 + i, d0 + l);
+            pad_[l] = (E)__ldg(Bad + i * ND + l);
         }
 #pragma unroll
         for (int j = 0; j < NB; ++j) {
@@ -438,7 +448,7 @@ __device__ __forceinline__ void scatter_async(const E* __restrict__ e, size_t st
             issue(slab + NBUF - 1);
             cp_async_wait<NBUF - 1>();  // this thread's copies of `slab` have landed
             const E* es = eb + (slab % NBUF) * SLAB * T;
-            const E pab = Pm(a0 + i, b0 + j);
+            const E pab = (E)__ldg(Bab + i * NB + j);
 #pragma unroll
             for (int k = 0; k < NC; ++k) {
                 const E pbc = pk[(j * NC + k) * T];
@@ -500,8 +510,9 @@ __global__ void __launch_bounds__(ND_THREADS, sizeof(E) == 4 ? 3 : 2) k_scatter_
             nsc = 1;
             const double s = (bra.sa == bra.sb ? 0.5 : 1.0) * (ket.sa == ket.sb ? 0.5 : 1.0);
             extern __shared__ __align__(16) double hf_scat_smem[];
-            scatter_async<NA, NB, NC, ND, E>(reinterpret_cast<const E*>(a.out) + t, a.stride, s, bra, ket, a.P,
-                                             a.G, a.nb, a.jonly != 0, reinterpret_cast<E*>(hf_scat_smem));
+            scatter_async<NA, NB, NC, ND, E>(reinterpret_cast<const E*>(a.out) + t, a.stride, s, bra, ket, a.Pb,
+                                             a.boff, a.nsh, a.G, a.nb, a.jonly != 0,
+                                             reinterpret_cast<E*>(hf_scat_smem));
         }
     }
     if (a.stats) warp_add_stats(a.stats, nsc, npr, a.f32 ? nsc : 0ull);

@@ -242,6 +242,18 @@ __global__ void k_offsets(OffsetArgs o, ScreenSub* __restrict__ subs, const unsi
     ncls[2 * c + 1] = n32;
 }
 
+// The density in shell-pair blocks: block (s1, s2) holds P[r][c] for the
+// functions r of shell s1 and c of shell s2, row-major, at boff[s1*nsh+s2].
+// Rows the scatter reads become contiguous (one element per column before).
+__global__ void k_pblock(const double* __restrict__ P, double* __restrict__ Pb, const int2* __restrict__ aomap,
+                         const int* __restrict__ nfsh, const int* __restrict__ boff, int nb, int nsh) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)nb * nb) return;
+    const int r = (int)(t % nb), c = (int)(t / nb);
+    const int2 mr = aomap[r], mc = aomap[c];  // (shell, function within the shell)
+    Pb[boff[mr.x * nsh + mc.x] + mr.y * nfsh[mc.x] + mc.y] = P[t];
+}
+
 // FMA-chain throughput probe: 8 independent chains per thread so the FP64 and
 // FP32 pipes, not latency, bound it.  Used to state the FP64/FP32 roofline.
 template <typename T>
@@ -334,6 +346,10 @@ struct hfgpu_handle {
     long long graph_launches = 0;       // kernels in the captured build
     OffsetArgs offs{};                  // sub-class ranges / list regions per class
     unsigned long long* d_ncls = nullptr;  // [2 * NCLS] surviving quartets (FP64, FP32) per class
+    double* d_Pb = nullptr;             // density in shell-pair blocks (nb x nb)
+    int* d_boff = nullptr;              // block offsets (nsh x nsh)
+    int2* d_aomap = nullptr;            // per function: (shell, index within the shell)
+    int* d_nfsh = nullptr;              // functions per shell
     cudaGraph_t graph = nullptr;        // captured full build (hfgpu_graph_capture)
     cudaGraphExec_t gexec = nullptr;
     const void* gkey_f = nullptr;       // what the capture was recorded with
@@ -729,6 +745,9 @@ int run_staged(hfgpu_handle* h, int c, int prec, long long n, const double* P, d
         a.stride = st;
         a.nroles = prec ? K.nrole_b32 : K.nrole_b;
         a.P = P;
+        a.Pb = h->d_Pb;
+        a.boff = h->d_boff;
+        a.nsh = h->nsh;
         a.G = h->d_G;
         a.nb = h->nb;
         a.thr = thr;
@@ -795,6 +814,13 @@ int run_non_diag(hfgpu_handle* h, const double* P, double thr, int jonly, double
         HF_CHECK(cudaMemsetAsync(h->d_cnt, 0, cbytes, h->stream));
         ++h->launches;
         k_screen<1><<<blocks, 256, 0, h->stream>>>(sa);  // compacted write
+        HF_CHECK(cudaGetLastError());
+    }
+    {  // the density in shell-pair blocks for the staged scatter
+        const long long n = (long long)h->nb * h->nb;
+        ++h->launches;
+        k_pblock<<<(int)((n + 255) / 256), 256, 0, h->stream>>>(P, h->d_Pb, h->d_aomap, h->d_nfsh, h->d_boff, h->nb,
+                                                                h->nsh);
         HF_CHECK(cudaGetLastError());
     }
     if (!capture) {
@@ -943,6 +969,10 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
     rc |= dalloc(&h->d_cnt, 2 * NCLS);
     rc |= dalloc(&h->d_stats, NCLS);
     rc |= dalloc(&h->d_ncls, 2 * NCLS);
+    rc |= dalloc(&h->d_Pb, nb2);
+    rc |= dalloc(&h->d_boff, (size_t)h->nsh * h->nsh);
+    rc |= dalloc(&h->d_aomap, (size_t)h->nb);
+    rc |= dalloc(&h->d_nfsh, (size_t)h->nsh);
     for (int t = 0; t < NPT; ++t) {
         size_t n = h->pairs[t].size();
         rc |= dalloc(&h->d_pairs[t], n);
@@ -975,6 +1005,25 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
     h->hprims = prims;
     if (ce == cudaSuccess) ce = up(h->d_boys, bt.data(), bt.size() * sizeof(double));
     if (ce == cudaSuccess) ce = up(h->d_boysf, btf.data(), btf.size() * sizeof(float));
+    {  // shell-pair block layout of the density
+        auto nf = [](int t) { return t == HFGPU_SHELL_S ? 1 : t == HFGPU_SHELL_P ? 3 : t == HFGPU_SHELL_D ? 5 : 4; };
+        std::vector<int> nfsh(h->nsh), boff((size_t)h->nsh * h->nsh);
+        std::vector<int2> aomap(h->nb, make_int2(0, 0));
+        for (int a = 0; a < h->nsh; ++a) {
+            nfsh[a] = nf(h->shtyp[a]);
+            for (int i = 0; i < nfsh[a] && h->aosh[a] + i < h->nb; ++i) aomap[h->aosh[a] + i] = make_int2(a, i);
+        }
+        long long off = 0;
+        for (int a = 0; a < h->nsh; ++a)
+            for (int b = 0; b < h->nsh; ++b) {
+                boff[(size_t)a * h->nsh + b] = (int)off;
+                off += (long long)nfsh[a] * nfsh[b];
+            }
+        if (off != (long long)h->nb * h->nb) ce = cudaErrorInvalidValue;  // the shells must tile the basis
+        if (ce == cudaSuccess) ce = up(h->d_nfsh, nfsh.data(), nfsh.size() * sizeof(int));
+        if (ce == cudaSuccess) ce = up(h->d_boff, boff.data(), boff.size() * sizeof(int));
+        if (ce == cudaSuccess) ce = up(h->d_aomap, aomap.data(), aomap.size() * sizeof(int2));
+    }
     for (int t = 0; t < NPT && ce == cudaSuccess; ++t) {
         std::vector<GPair> gp(h->pairs[t].size());
         for (size_t i = 0; i < gp.size(); ++i) gp[i] = h->pairs[t][i].g;
@@ -1030,7 +1079,7 @@ int hfgpu_finalize(hfgpu_handle* h) {
     if (h->graph) cudaGraphDestroy(h->graph);
     void* bufs[] = {h->d_shtyp, h->d_aosh, h->d_psoa, h->d_apsoa, h->d_boys, h->d_boysf, h->d_P, h->d_F, h->d_G,
                     h->d_md, h->d_subs, h->d_q, h->d_cnt, h->d_stats, h->d_scratch, h->d_dscratch,
-                    h->d_ncls};
+                    h->d_ncls, h->d_Pb, h->d_boff, h->d_aomap, h->d_nfsh};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (int t = 0; t < NPT; ++t) {
@@ -1303,7 +1352,8 @@ int hfgpu_device_bytes(const hfgpu_handle* h, size_t* bytes) {
     if (!h || !bytes) return set_err(HFGPU_ERR_ARG, "null argument");
     size_t b = 0;
     const size_t nb2 = (size_t)h->nb * h->nb;
-    b += 3 * nb2 * sizeof(double);                            // P, F, G
+    b += 4 * nb2 * sizeof(double);                            // P, F, G, blocked P
+    b += ((size_t)h->nsh * h->nsh + 2 * (size_t)h->nb + h->nsh) * sizeof(int);
     b += (size_t)h->nsh * h->nsh * sizeof(double);            // maxdm
     b += 2 * (size_t)h->nsh * sizeof(int);
     b += 8 * h->hprims.size() * sizeof(double);               // all-pairs primitives
