@@ -269,7 +269,7 @@ def run_reference(args):
                       "e2e": {"value": v, "unit": "builds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
-LLDL_DRAM_BYTES_PER_QUARTET = 2974.0  # (176.3 + 3750.5 MB read + 112.2 MB written) / 5 builds / 271,664 quartets
+LLDL_DRAM_BYTES_PER_QUARTET = 2811.0  # (130.4 + 3649.3 MB read + 37.9 MB written) / 5 builds / 271,664 quartets
 
 
 def main():
