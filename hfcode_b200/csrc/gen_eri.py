@@ -574,7 +574,9 @@ MAXR = 64           # role slots in ClassKernels
 
 # Per-class shape overrides (measured on the device; see tuning.json beside
 # this file): {"<tag>": {"acc_max": .., "out_max": .., "max_roles2": ..,
-# "acc_group": .., "out_group3": ..}}.  HFGPU_TUNING names another file.
+# "acc_group": .., "out_group3": .., "staged": true}}; "staged" keeps a
+# one-role class on the staged path (outputs through scratch, staged scatter)
+# instead of the direct one.  HFGPU_TUNING names another file.
 _TUNING_FILE = os.environ.get("HFGPU_TUNING") or os.path.join(os.path.dirname(os.path.abspath(__file__)),
                                                               "tuning.json")
 
@@ -635,7 +637,7 @@ def class_source(ci: int, bi: int, ki: int):
     info = {"name": f"{g.A}{g.B}|{g.C}{g.D}", "tag": g.tag, "L": g.L, "nout": g.nout,
             "flops_prim": g.flops_prim, "flops_quartet": g.flops_quartet,
             "vrr_terms": g.nvrr, "hrr_terms": g.nhrr}
-    if len(roles) == 1:
+    if len(roles) == 1 and not prm.get("staged", False):
         mode = "direct"
         code, _ = g.emit_role(g.name, roles[0])
         code32, _ = g32.emit_role(g32.name, roles[0])
