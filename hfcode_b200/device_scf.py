@@ -174,27 +174,19 @@ class DeviceSCF:
             return
         g = self._graphs.get(key)
         if g is None:
-            # warm up once on a side stream (cuBLAS workspaces), then record
-            side = torch.cuda.Stream(self.dev)
-            side.wait_stream(torch.cuda.current_stream(self.dev))
-            state = [t.clone() for t in self._state()]
-            with torch.cuda.stream(side):
-                self._build(kind, thr, fdifffac, cut)
-                self._post(loose)
-            torch.cuda.current_stream(self.dev).wait_stream(side)
-            for t, s in zip(self._state(), state):
-                t.copy_(s)
+            # the first cycle of a kind runs eagerly (which also warms up the
+            # libraries) and is then recorded, without running it again, for
+            # the later cycles of that kind
+            self._build(kind, thr, fdifffac, cut)
+            self._post(loose)
             from .fock import DEVICE_LOCK
             g = torch.cuda.CUDAGraph()
             with DEVICE_LOCK, torch.cuda.graph(g, capture_error_mode="thread_local"):
                 self._build(kind, thr, fdifffac, cut)
                 self._post(loose)
             self._graphs[key] = g
+            return
         g.replay()
-
-    def _state(self):
-        return [self.P, self.Pold, self.Pnew, self.F, self.Fold, self.dF, self.R, self.FO, self.eo, self.n,
-                self.diis, self.A, self.rhs, self.status, self.out]
 
     # ------------------------------------------------------------ protocol
     def run(self, p_guess: np.ndarray, maxiter: int = 25, conv: float = 1e-5, conve: float = 5e-8,
