@@ -25,6 +25,11 @@ def system(name: str):
 def _system(name: str):
     if name == "water":
         mol, bas = molecules.water(), basis.load_basis("STO-3G")
+    elif name == "h2":  # s shells only: the SS|SS class alone
+        mol, bas = basis.Molecule(["H", "H"], np.array([[0.0, 0.0, 0.0], [0.0, 0.0, 0.74]])), \
+            basis.load_basis("STO-3G")
+    elif name == "ne":  # one centre: every quartet has AB = CD = PQ = 0 (Boys at T = 0)
+        mol, bas = basis.Molecule(["Ne"], np.zeros((1, 3))), basis.load_basis("6-31G(d)")
     elif name == "benzene":
         mol, bas = molecules.benzene(), basis.load_basis("6-31G(d)")
     elif name == "c60":

@@ -34,7 +34,8 @@ def oracle_counts_by_gpu_class(orc):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["water", "alkane1", "alkane2", "benzene", "water_sp", "alkane2_sp", "alkane2_mix"])
+@pytest.mark.parametrize("name", ["water", "alkane1", "alkane2", "benzene", "water_sp", "alkane2_sp", "alkane2_mix",
+                                  "h2", "ne"])
 def test_fock_build_parity(name):
     from hfcode_b200.fock import FockBuilder
     _, _, sh, p0 = system(name)
