@@ -381,7 +381,7 @@ template <int NA, int NB, int NC, int ND, typename E>
 __device__ __forceinline__ void scatter_async(const E* __restrict__ e, size_t st, double s, const GPair& bra,
                                               const GPair& ket, const double* __restrict__ Pb,
                                               const int* __restrict__ boff, int nsh,
-                                              double* __restrict__ G, int nb, bool jonly, E* sm) {
+                                              double* __restrict__ G, int nb, bool jonly, bool act, E* sm) {
     constexpr int T = ND_THREADS, SLAB = NC * ND, NS = NA * NB;
     constexpr int NBUF = scat_nbuf(NA, NB, NC, ND, (int)sizeof(E));
     const int tid = threadIdx.x;
@@ -395,6 +395,12 @@ __device__ __forceinline__ void scatter_async(const E* __restrict__ e, size_t st
     const double* __restrict__ Bbd = Pb + __ldg(boff + bra.sb * nsh + ket.sb);
     const double* __restrict__ Bcd = Pb + __ldg(boff + ket.sa * nsh + ket.sb);
     auto Ga = [&](int r, int c) { return G + r + (size_t)c * nb; };
+    // consecutive quartets mostly share their bra pair: when the whole warp
+    // does, its J_ab sums (same addresses) are reduced across the warp and
+    // added once
+    const unsigned long long bkey = ((unsigned long long)bra.aoa << 32) | (unsigned)bra.aob;
+    const bool wuni = __all_sync(0xffffffffu, bkey == __shfl_sync(0xffffffffu, bkey, 0));
+    const int lane = threadIdx.x & 31;
     E* eb = sm + tid;                      // [NBUF][SLAB][T], this thread's column
     E* pk = sm + NBUF * SLAB * T + tid;    // [NB*NC] P_bc then [NB*ND] P_bd
     auto issue = [&](int slab) {
@@ -467,8 +473,17 @@ __device__ __forceinline__ void scatter_async(const E* __restrict__ e, size_t st
             }
         }
 #pragma unroll
-        for (int j = 0; j < NB; ++j) atomicAdd(Ga(a0 + i, b0 + j), (double)(s2 * jab[j]));
-        if (!jonly) {
+        for (int j = 0; j < NB; ++j) {
+            double v = act ? (double)(s2 * jab[j]) : 0.0;
+            if (wuni) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0) atomicAdd(Ga(a0 + i, b0 + j), v);
+            } else if (act) {
+                atomicAdd(Ga(a0 + i, b0 + j), v);
+            }
+        }
+        if (!jonly && act) {
 #pragma unroll
             for (int k = 0; k < NC; ++k) atomicAdd(Ga(a0 + i, c0 + k), (double)(hs * kac[k]));
 #pragma unroll
@@ -476,6 +491,7 @@ __device__ __forceinline__ void scatter_async(const E* __restrict__ e, size_t st
         }
     }
     cp_async_wait<0>();
+    if (!act) return;
 #pragma unroll
     for (int k = 0; k < NC; ++k)
 #pragma unroll
@@ -498,23 +514,26 @@ __device__ __forceinline__ void scatter_async(const E* __restrict__ e, size_t st
 template <int NA, int NB, int NC, int ND, typename E = double>
 __global__ void __launch_bounds__(ND_THREADS, sizeof(E) == 4 ? 3 : 2) k_scatter_staged(StagedArgs a) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    unsigned long long nsc = 0, npr = 0;
-    if (t < staged_count(a)) {
-        double m = 0.0;
-        for (int r = 0; r < a.nroles; ++r) m = fmax(m, a.mx[(size_t)r * a.stride + t]);
-        const uint2 q = staged_quartet(a, t);
-        const GPair bra = a.bra[q.x];
-        const GPair ket = a.ket[q.y];
-        npr = (unsigned long long)(bra.np * ket.np);
-        if (!(m < a.thr)) {
-            nsc = 1;
-            const double s = (bra.sa == bra.sb ? 0.5 : 1.0) * (ket.sa == ket.sb ? 0.5 : 1.0);
-            extern __shared__ __align__(16) double hf_scat_smem[];
-            scatter_async<NA, NB, NC, ND, E>(reinterpret_cast<const E*>(a.out) + t, a.stride, s, bra, ket, a.Pb,
-                                             a.boff, a.nsh, a.G, a.nb, a.jonly != 0,
-                                             reinterpret_cast<E*>(hf_scat_smem));
-        }
-    }
+    const int cnt = staged_count(a);
+    const int w0 = t - (threadIdx.x & 31);  // first quartet of this warp
+    if (w0 >= cnt) return;                  // a warp with no quartet (whole warps only)
+    // every lane of the warp runs the scatter so that the J_ab sums can be
+    // reduced across the warp; a lane past the end works on the warp's first
+    // quartet and writes nothing
+    const bool valid = t < cnt;
+    const int tq = valid ? t : w0;
+    double m = 0.0;
+    for (int r = 0; r < a.nroles; ++r) m = fmax(m, a.mx[(size_t)r * a.stride + tq]);
+    const uint2 q = staged_quartet(a, tq);
+    const GPair bra = a.bra[q.x];
+    const GPair ket = a.ket[q.y];
+    const bool act = valid && !(m < a.thr);  // fock_build_non_diag.f90:69
+    const unsigned long long nsc = act ? 1ull : 0ull;
+    const unsigned long long npr = valid ? (unsigned long long)(bra.np * ket.np) : 0ull;
+    const double s = (bra.sa == bra.sb ? 0.5 : 1.0) * (ket.sa == ket.sb ? 0.5 : 1.0);
+    extern __shared__ __align__(16) double hf_scat_smem[];
+    scatter_async<NA, NB, NC, ND, E>(reinterpret_cast<const E*>(a.out) + tq, a.stride, s, bra, ket, a.Pb, a.boff,
+                                     a.nsh, a.G, a.nb, a.jonly != 0, act, reinterpret_cast<E*>(hf_scat_smem));
     if (a.stats) warp_add_stats(a.stats, nsc, npr, a.f32 ? nsc : 0ull);
 }
 
