@@ -54,8 +54,10 @@ def build(jobs: int = 0, verbose: bool = True) -> str:
               os.path.join(CSRC, "scatter.cuh"),
               os.path.join(HERE, "..", "include", "hfgpu.h"),
               os.path.join(HERE, "..", "include", "hfgpu_basis.h"),
+              os.path.join(HERE, "..", "include", "hfgpu_ingest.h"),
               os.path.join(CSRC, "generated", "class_table.inc")]
-    srcs = [os.path.join(CSRC, "hfgpu.cu"), os.path.join(CSRC, "onee.cu")] + sorted(gen_srcs)
+    srcs = [os.path.join(CSRC, "hfgpu.cu"), os.path.join(CSRC, "onee.cu"),
+            os.path.join(CSRC, "ingest.cpp")] + sorted(gen_srcs)
     objs = [os.path.join(BUILD, os.path.splitext(os.path.basename(s))[0] + ".o") for s in srcs]
     jobs = jobs or max(1, min(len(srcs), os.cpu_count() or 4))
     with cf.ThreadPoolExecutor(jobs) as ex:

@@ -4,7 +4,7 @@ import ctypes
 import os
 import re
 
-from hfcode_b200 import fock
+from hfcode_b200 import fock, ingest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -27,7 +27,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_python_binding_lists_all_exports():
-    assert set(fock.EXPORTS) >= declared_symbols()
+    assert set(fock.EXPORTS) | set(ingest.EXPORTS) >= declared_symbols()
 
 
 def test_init_rejects_bad_arguments_without_gpu_compute():
