@@ -112,3 +112,45 @@ def test_calls_before_initial_diag_are_rejected():
     with pytest.raises(HfgpuError):
         fb.fock_build_non_diag(np.zeros((sh.nb, sh.nb)), p0, 1e-10)
     fb.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["zero_density", "one_atom_block", "thr_zero", "thr_huge"])
+def test_edge_densities_and_thresholds(case):
+    """Ragged and degenerate inputs: P = 0 and a threshold above every bound
+    (every quartet screened out: empty class lists, F left exactly as it
+    was), a density with one atom's block only (most shell pairs screened
+    out, a few classes active), and thr = 0 (nothing dropped by either
+    screen).  Parity and the per-class counts against the oracle."""
+    from hfcode_b200.fock import FockBuilder
+    name = "alkane1" if case == "thr_zero" else "benzene"
+    _, _, sh, p0 = system(name)
+    nb = sh.nb
+    fb = FockBuilder(sh)
+    orc = pyoracle.Oracle(sh)
+    fb.fock_build_initial_diag(np.zeros((nb, nb)), p0, 1e-10)
+    orc.fock_build_initial_diag(np.zeros((nb, nb)), p0, 1e-10)
+    thr = {"thr_zero": 0.0, "thr_huge": 1e3}.get(case, 1e-10)
+    if case == "zero_density":
+        p = np.zeros((nb, nb))
+    elif case == "one_atom_block":
+        n0 = int(sh.nbfsat[0])
+        p = np.zeros((nb, nb))
+        p[:n0, :n0] = perturbed_density(p0, 4)[:n0, :n0]
+    else:
+        p = perturbed_density(p0, 4)
+    h = np.random.default_rng(5).normal(size=(nb, nb))
+    h = h + h.T
+    fg, fo = h.copy(order="F"), h.copy(order="F")
+    for f, b in ((fg, fb), (fo, orc)):
+        b.fock_build_diag(f, p, thr)
+        b.fock_build_non_diag(f, p, thr)
+    st = fb.class_stats()
+    assert np.array_equal(st["pass"], oracle_counts_by_gpu_class(orc))
+    if case in ("zero_density", "thr_huge"):
+        assert st["pass"].sum() == 0
+        assert np.array_equal(fg, h)
+    else:
+        assert st["pass"].sum() > 0
+        assert np.max(np.abs(fg - fo)) < TOL
+    fb.close()
