@@ -588,7 +588,7 @@ struct ClassKernels {
     StagedKernel sa64[MAXR], sa32[MAXR], sb64[MAXR], sb32[MAXR], scat;
     StagedKernel dscat0, dscat1;  // staged diagonal builders (classes (X|X))
     int scat_smem;                // dynamic shared memory of scat (bytes)
-    StagedKernel scat32;          // staged2: scatter of FP32 chunks (float rows), or nullptr
+    StagedKernel scat32;          // scatter of FP32 chunks (float rows), or nullptr
     int scat32_smem;
     int bi, ki, L, nout;
 };

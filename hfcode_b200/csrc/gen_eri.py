@@ -474,18 +474,20 @@ class ClassGen:
         out = [f"// ({self.A}{self.B}|{self.C}{self.D}) accumulators ({len(keys)}): VRR {vst['vrr']} terms "
                f"({vst['order']}-first)",
                f"__device__ __forceinline__ void {fname}(const GPair& bra, const GPair& ket,",
-               f"    const PrimSoA& prims, const {ft}* __restrict__ btab, double* __restrict__ dst, "
+               f"    const PrimSoA& prims, const {ft}* __restrict__ btab, {ft}* __restrict__ dst, "
                f"size_t stride)",
                "{"]
         out += vlines
-        out += [f"    dst[{k} * stride] = (double){acc[key]};" for k, key in enumerate(keys)]
+        out += [f"    dst[{k} * stride] = {acc[key]};" for k, key in enumerate(keys)]
         out.append("}")
         return "\n".join(out), vst
 
     def emit_hrr_role(self, fname: str, outs: List[int], keyidx: Dict[Tuple, int]):
         """Stage-B device function: outputs `outs` from the accumulators in
         src[keyidx[key] * stride], written to dst[r * stride]; returns
-        max |value|."""
+        max |value|.  Accumulators, arithmetic and outputs are in the
+        generator's type (FP32 chunks keep FP32 throughout)."""
+        ft = self.ft
         loaded = {}
         lines = []
 
@@ -493,18 +495,18 @@ class ClassGen:
             if key not in loaded:
                 nm = f"L{keyidx[key]}"
                 loaded[key] = nm
-                lines.append(f"    const double {nm} = __ldg(src + {keyidx[key]} * stride);")
+                lines.append(f"    const {ft} {nm} = __ldg(src + {keyidx[key]} * stride);")
             return loaded[key]
 
-        hlines, vals, hst = self._hrr_block(outs, leaf, "double")
+        hlines, vals, hst = self._hrr_block(outs, leaf, ft)
         out = [f"// ({self.A}{self.B}|{self.C}{self.D}) outputs {outs[0]}..{outs[-1]} ({len(outs)}) from accumulators",
                f"__device__ __forceinline__ double {fname}(const GPair& bra, const GPair& ket,",
-               f"    const double* __restrict__ src, double* __restrict__ dst, size_t stride)",
+               f"    const {ft}* __restrict__ src, {ft}* __restrict__ dst, size_t stride)",
                "{"]
         out += hlines[:2] + lines + hlines[2:]
         out.append("    double mx = 0.0;")
         for r, v in enumerate(vals):
-            out.append(f"    {{ const double v = {v}; dst[{r} * stride] = v; mx = fmax(mx, fabs(v)); }}")
+            out.append(f"    {{ const {ft} v = {v}; dst[{r} * stride] = v; mx = fmax(mx, fabs((double)v)); }}")
         out.append("    return mx;")
         out.append("}")
         return "\n".join(out), hst
@@ -727,33 +729,41 @@ __global__ void __launch_bounds__(ND_THREADS, F32 ? 3 : 2) k_sa_{g.tag}_r{r}(Sta
     const uint2 q = staged_quartet(a, t);
     const GPair bra = a.bra[q.x];
     const GPair ket = a.ket[q.y];
-    if constexpr (F32) acc_{g.tag}_f32_r{r}(bra, ket, a.prims, sboys, a.acc + (size_t){base} * a.stride + t, a.stride);
-    else acc_{g.tag}_r{r}(bra, ket, a.prims, sboys, a.acc + (size_t){base} * a.stride + t, a.stride);
+    // FP32 chunks keep their accumulators in FP32
+    Real* dst = reinterpret_cast<Real*>(a.acc) + (size_t){base} * a.stride + t;
+    if constexpr (F32) acc_{g.tag}_f32_r{r}(bra, ket, a.prims, sboys, dst, a.stride);
+    else acc_{g.tag}_r{r}(bra, ket, a.prims, sboys, dst, a.stride);
 }}""")
             base += len(gr)
         og = prm["out_group3"]
         outroles = [list(range(i, min(i + og, g.nout))) for i in range(0, g.nout, og)]
         for r, outs in enumerate(outroles):
             code, _ = g.emit_hrr_role(f"hrr_{g.tag}_r{r}", outs, keyidx)
-            funcs.append(code)
-            kern.append(f"""
-__global__ void __launch_bounds__(ND_THREADS) k_sb_{g.tag}_r{r}(StagedArgs a) {{
+            code32, _ = g32.emit_hrr_role(f"hrr_{g.tag}_f32_r{r}", outs, keyidx)
+            funcs += [code, code32]
+            for kname, fname, real in ((f"k_sb_{g.tag}_r{r}", f"hrr_{g.tag}_r{r}", "double"),
+                                       (f"k_sbf_{g.tag}_r{r}", f"hrr_{g.tag}_f32_r{r}", "float")):
+                kern.append(f"""
+__global__ void __launch_bounds__(ND_THREADS) {kname}(StagedArgs a) {{
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= staged_count(a)) return;
     const uint2 q = staged_quartet(a, t);
     const GPair bra = a.bra[q.x];
     const GPair ket = a.ket[q.y];
     a.mx[(size_t){r} * a.stride + t] =
-        hrr_{g.tag}_r{r}(bra, ket, a.acc + t, a.out + (size_t){outs[0]} * a.stride + t, a.stride);
+        {fname}(bra, ket, reinterpret_cast<const {real}*>(a.acc) + t,
+                reinterpret_cast<{real}*>(a.out) + (size_t){outs[0]} * a.stride + t, a.stride);
 }}""")
         reg.append(f"    k->mode = 2;\n    k->nacc = {len(keyidx)};\n    k->nrole_a = {len(groups)};\n"
                    f"    k->nrole_b = {len(outroles)};\n    k->nrole_b32 = {len(outroles)};")
         for r in range(len(groups)):
             reg.append(f"    k->sa64[{r}] = k_sa_{g.tag}_r{r}<false>;\n    k->sa32[{r}] = k_sa_{g.tag}_r{r}<true>;")
         for r in range(len(outroles)):
-            reg.append(f"    k->sb64[{r}] = k_sb_{g.tag}_r{r};\n    k->sb32[{r}] = k_sb_{g.tag}_r{r};")
+            reg.append(f"    k->sb64[{r}] = k_sb_{g.tag}_r{r};\n    k->sb32[{r}] = k_sbf_{g.tag}_r{r};")
         reg.append(f"    k->scat = k_scatter_staged<{NA}, {NB}, {NC}, {ND}>;\n"
-                   f"    k->scat_smem = scat_smem_bytes({NA}, {NB}, {NC}, {ND});")
+                   f"    k->scat_smem = scat_smem_bytes({NA}, {NB}, {NC}, {ND});\n"
+                   f"    k->scat32 = k_scatter_staged<{NA}, {NB}, {NC}, {ND}, float>;\n"
+                   f"    k->scat32_smem = scat_smem_bytes({NA}, {NB}, {NC}, {ND}, 4);")
         if bi == ki:
             reg.append(f"    k->diag0 = nullptr;\n    k->diag1 = nullptr;")
             reg.append(f"    k->dscat0 = k_scatter_diag<{NA}, {NB}, 0>;\n    k->dscat1 = k_scatter_diag<{NA}, {NB}, 1>;")
@@ -905,13 +915,17 @@ def main(outdir: str):
         else:
             nacc = sum(len(g) for g in info["acc_groups"])
             lines.append(f"    static double acc[{nacc}];")
+            lines.append(f"    static float accf[{nacc}];")
             base = 0
             for r, gr in enumerate(info["acc_groups"]):
-                lines.append(f"    if (f32) acc_{tag}_f32_r{r}(b, k, p, tf, acc + {base}, 1);")
+                lines.append(f"    if (f32) acc_{tag}_f32_r{r}(b, k, p, tf, accf + {base}, 1);")
                 lines.append(f"    else acc_{tag}_r{r}(b, k, p, t, acc + {base}, 1);")
                 base += len(gr)
             for r, outs in enumerate(info["role_outs"]):
-                lines.append(f"    hrr_{tag}_r{r}(b, k, acc, out + {outs[0]}, 1);")
+                n = len(outs)
+                lines.append(f"    if (f32) {{ float of[{n}]; hrr_{tag}_f32_r{r}(b, k, accf, of, 1);")
+                lines.append(f"      for (int i = 0; i < {n}; ++i) out[{outs[0]} + i] = of[i]; }}")
+                lines.append(f"    else hrr_{tag}_r{r}(b, k, acc, out + {outs[0]}, 1);")
         lines.append("}")
         # the J/K scatter of a full block with stride 1
         na, nb_, nc, nd = info["dims"]
