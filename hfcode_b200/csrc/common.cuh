@@ -585,6 +585,7 @@ struct ClassKernels {
     int dg_threads, dg_ppb;   // block size and pairs per block (diag)
     int nacc, nrole_a, nrole_b;
     int nrole_b32;            // output roles of the FP32 chunks (staged2: larger roles)
+    int nrole_a32;            // accumulator roles of the FP32 chunks (staged3: larger groups)
     StagedKernel sa64[MAXR], sa32[MAXR], sb64[MAXR], sb32[MAXR], scat;
     StagedKernel dscat0, dscat1;  // staged diagonal builders (classes (X|X))
     int scat_smem;                // dynamic shared memory of scat (bytes)

@@ -590,6 +590,7 @@ def class_params(tag: str) -> dict:
         with open(_TUNING_FILE) as fh:
             prm.update(json.load(fh).get(tag, {}))
     prm.setdefault("acc_max32", 2 * prm["acc_max"])
+    prm.setdefault("acc_group32", 2 * prm["acc_group"])
     prm.setdefault("out_max32", 2 * prm["out_max"])
     return prm
 
@@ -712,29 +713,29 @@ __global__ void __launch_bounds__(ND_THREADS, 2) {kname}(StagedArgs a) {{
         for gr in groups:
             for key in gr:
                 keyidx[key] = len(keyidx)
-        base = 0
-        for r, gr in enumerate(groups):
-            code, _ = g.emit_acc_role(f"acc_{g.tag}_r{r}", gr)
-            code32, _ = g32.emit_acc_role(f"acc_{g.tag}_f32_r{r}", gr)
-            funcs += [code, code32]
-            kern.append(f"""
-template <bool F32>
-__global__ void __launch_bounds__(ND_THREADS, F32 ? 3 : 2) k_sa_{g.tag}_r{r}(StagedArgs a) {{
-    using Real = typename std::conditional<F32, float, double>::type;
-    const Real* __restrict__ sboys;  // Boys table of order L, through the L1 cache
-    if constexpr (F32) sboys = a.boysf + (size_t){g.L} * BOYS_BLK;
-    else sboys = a.boys + (size_t){g.L} * BOYS_BLK;
+        # FP32 values take half the registers: the FP32 stage-A roles take
+        # acc_group32 accumulators (consecutive FP64 groups merged), so fewer
+        # of them repeat the primitive loop; the accumulator layout is the same
+        per32 = max(1, prm["acc_group32"] // prm["acc_group"])
+        groups32 = [sum(groups[i:i + per32], []) for i in range(0, len(groups), per32)]
+        for gset, gen, real, kpre in ((groups, g, "double", "k_sa"), (groups32, g32, "float", "k_saf")):
+            base = 0
+            tab = "a.boysf" if real == "float" else "a.boys"
+            for r, gr in enumerate(gset):
+                fname = f"acc_{g.tag}{'_f32' if real == 'float' else ''}_r{r}"
+                code, _ = gen.emit_acc_role(fname, gr)
+                funcs.append(code)
+                kern.append(f"""
+__global__ void __launch_bounds__(ND_THREADS, 2) {kpre}_{g.tag}_r{r}(StagedArgs a) {{
+    const {real}* __restrict__ sboys = {tab} + (size_t){g.L} * BOYS_BLK;  // Boys table of order L, through L1
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= staged_count(a)) return;
     const uint2 q = staged_quartet(a, t);
     const GPair bra = a.bra[q.x];
     const GPair ket = a.ket[q.y];
-    // FP32 chunks keep their accumulators in FP32
-    Real* dst = reinterpret_cast<Real*>(a.acc) + (size_t){base} * a.stride + t;
-    if constexpr (F32) acc_{g.tag}_f32_r{r}(bra, ket, a.prims, sboys, dst, a.stride);
-    else acc_{g.tag}_r{r}(bra, ket, a.prims, sboys, dst, a.stride);
+    {fname}(bra, ket, a.prims, sboys, reinterpret_cast<{real}*>(a.acc) + (size_t){base} * a.stride + t, a.stride);
 }}""")
-            base += len(gr)
+                base += len(gr)
         og = prm["out_group3"]
         outroles = [list(range(i, min(i + og, g.nout))) for i in range(0, g.nout, og)]
         for r, outs in enumerate(outroles):
@@ -755,9 +756,12 @@ __global__ void __launch_bounds__(ND_THREADS) {kname}(StagedArgs a) {{
                 reinterpret_cast<{real}*>(a.out) + (size_t){outs[0]} * a.stride + t, a.stride);
 }}""")
         reg.append(f"    k->mode = 2;\n    k->nacc = {len(keyidx)};\n    k->nrole_a = {len(groups)};\n"
+                   f"    k->nrole_a32 = {len(groups32)};\n"
                    f"    k->nrole_b = {len(outroles)};\n    k->nrole_b32 = {len(outroles)};")
         for r in range(len(groups)):
-            reg.append(f"    k->sa64[{r}] = k_sa_{g.tag}_r{r}<false>;\n    k->sa32[{r}] = k_sa_{g.tag}_r{r}<true>;")
+            reg.append(f"    k->sa64[{r}] = k_sa_{g.tag}_r{r};")
+        for r in range(len(groups32)):
+            reg.append(f"    k->sa32[{r}] = k_saf_{g.tag}_r{r};")
         for r in range(len(outroles)):
             reg.append(f"    k->sb64[{r}] = k_sb_{g.tag}_r{r};\n    k->sb32[{r}] = k_sbf_{g.tag}_r{r};")
         reg.append(f"    k->scat = k_scatter_staged<{NA}, {NB}, {NC}, {ND}>;\n"
@@ -768,7 +772,8 @@ __global__ void __launch_bounds__(ND_THREADS) {kname}(StagedArgs a) {{
             reg.append(f"    k->diag0 = nullptr;\n    k->diag1 = nullptr;")
             reg.append(f"    k->dscat0 = k_scatter_diag<{NA}, {NB}, 0>;\n    k->dscat1 = k_scatter_diag<{NA}, {NB}, 1>;")
         info.update(roles=len(outroles), role_sizes=[len(x) for x in outroles], role_outs=outroles,
-                    acc_groups=[[[list(k[2]), list(k[3]), k[0], k[1]] for k in gr] for gr in groups])
+                    acc_groups=[[[list(k[2]), list(k[3]), k[0], k[1]] for k in gr] for gr in groups],
+                    acc_groups32=[[[list(k[2]), list(k[3]), k[0], k[1]] for k in gr] for gr in groups32])
         assert len(groups) <= MAXR and len(outroles) <= MAXR
     if mode == "staged2":
         assert len(roles) <= MAXR
@@ -918,8 +923,11 @@ def main(outdir: str):
             lines.append(f"    static float accf[{nacc}];")
             base = 0
             for r, gr in enumerate(info["acc_groups"]):
+                lines.append(f"    if (!f32) acc_{tag}_r{r}(b, k, p, t, acc + {base}, 1);")
+                base += len(gr)
+            base = 0
+            for r, gr in enumerate(info["acc_groups32"]):
                 lines.append(f"    if (f32) acc_{tag}_f32_r{r}(b, k, p, tf, accf + {base}, 1);")
-                lines.append(f"    else acc_{tag}_r{r}(b, k, p, t, acc + {base}, 1);")
                 base += len(gr)
             for r, outs in enumerate(info["role_outs"]):
                 n = len(outs)

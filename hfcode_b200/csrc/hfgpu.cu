@@ -755,7 +755,7 @@ int run_staged(hfgpu_handle* h, int c, int prec, long long n, const double* P, d
         a.f32 = prec;
         a.stats = h->d_stats + c;
         const int blocks = (m + ND_THREADS - 1) / ND_THREADS;
-        for (int r = 0; r < K.nrole_a; ++r) {
+        for (int r = 0; r < (prec ? K.nrole_a32 : K.nrole_a); ++r) {
             ++h->launches;
             (prec ? K.sa32[r] : K.sa64[r])<<<blocks, ND_THREADS, 0, stream>>>(a);
             HF_CHECK(cudaGetLastError());
