@@ -385,10 +385,13 @@ class ClassGen:
         nbracket = sum(line.count(" - r") for line in em.lines)
         return out, acc, {"vrr": vrr.nops, "bracket": nbracket, "acc": len(acc), "order": vrr.order}
 
-    def _hrr_block(self, outs, leaf, ft):
+    def _hrr_block(self, outs, leaf, ft, store=None):
         """HRR on ket and bra plus the spherical transform for `outs`;
-        leaf(key) names the contracted accumulator.  Returns (lines, value
-        expressions per output, stats)."""
+        leaf(key) names the contracted accumulator, or returns (name, line)
+        to have the line (its load) emitted where it is first used.  With
+        `store`, store(r, expr) is emitted right after output r's terms, so
+        each output leaves the registers as soon as it is formed.  Returns
+        (lines, value expressions per output, stats)."""
         cv = (lambda s: s) if ft == "double" else (lambda s: f"(float)({s})")
         lines = [f"    const {ft} AB0 = {cv('bra.A[0] - bra.B[0]')}, AB1 = {cv('bra.A[1] - bra.B[1]')}, "
                  f"AB2 = {cv('bra.A[2] - bra.B[2]')};",
@@ -403,6 +406,10 @@ class ClassGen:
                 return memo[key]
             if d == Z3:
                 r = leaf((bi, ki, e, c))
+                if isinstance(r, tuple):
+                    r, ln = r
+                    if ln:
+                        hem.raw(ln)
             else:
                 i = max(range(3), key=lambda k: (d[k], -k))
                 d1 = add(d, i, -1)
@@ -438,8 +445,11 @@ class ClassGen:
                 terms.append(v if coef == 1.0 else f"{fmt_coef(coef, ft)}*{v}")
             nsph += len(terms) - 1
             vals.append(" + ".join(terms))
+            if store is not None:
+                hem.raw(store(len(vals) - 1, vals[-1]))
+        nh = sum(1 for ln in hem.lines if ln.lstrip().startswith(f"const {ft} h"))
         lines += hem.lines
-        return lines, vals, {"hrr": len(hem.lines), "sph": nsph}
+        return lines, vals, {"hrr": nh, "sph": nsph}
 
     def needed_keys(self, outs):
         keys = set()
@@ -489,24 +499,28 @@ class ClassGen:
         generator's type (FP32 chunks keep FP32 throughout)."""
         ft = self.ft
         loaded = {}
-        lines = []
 
         def leaf(key):
+            # each accumulator is loaded where the recursion first needs it
+            # and each output is stored as soon as it is formed: hoisting
+            # every load to the top and every store to the end kept all of
+            # them live at once and spilled the d-heavy roles
             if key not in loaded:
                 nm = f"L{keyidx[key]}"
                 loaded[key] = nm
-                lines.append(f"    const {ft} {nm} = __ldg(src + {keyidx[key]} * stride);")
-            return loaded[key]
+                return nm, f"    const {ft} {nm} = __ldg(src + {keyidx[key]} * stride);"
+            return loaded[key], None
 
-        hlines, vals, hst = self._hrr_block(outs, leaf, ft)
+        def store(r, v):
+            return f"    {{ const {ft} v = {v}; dst[{r} * stride] = v; mx = fmax(mx, fabs((double)v)); }}"
+
+        hlines, vals, hst = self._hrr_block(outs, leaf, ft, store)
         out = [f"// ({self.A}{self.B}|{self.C}{self.D}) outputs {outs[0]}..{outs[-1]} ({len(outs)}) from accumulators",
                f"__device__ __forceinline__ double {fname}(const GPair& bra, const GPair& ket,",
                f"    const {ft}* __restrict__ src, {ft}* __restrict__ dst, size_t stride)",
-               "{"]
-        out += hlines[:2] + lines + hlines[2:]
-        out.append("    double mx = 0.0;")
-        for r, v in enumerate(vals):
-            out.append(f"    {{ const {ft} v = {v}; dst[{r} * stride] = v; mx = fmax(mx, fabs((double)v)); }}")
+               "{",
+               "    double mx = 0.0;"]
+        out += hlines
         out.append("    return mx;")
         out.append("}")
         return "\n".join(out), hst
