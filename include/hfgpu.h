@@ -161,7 +161,8 @@ int hfgpu_set_timing(hfgpu_handle* h, int on);
 
 /* Upper bound in bytes of the staged classes' scratch (chunks of quartets
  * through the accumulator/output roles); set before
- * hfgpu_fock_build_initial_diag.  Default: HFGPU_SCRATCH_MB or 6 GiB. */
+ * hfgpu_fock_build_initial_diag.  Default: HFGPU_SCRATCH_MB, else 24 GiB capped at
+ * a sixth of the device's memory. */
 int hfgpu_set_scratch_budget(hfgpu_handle* h, size_t bytes);
 
 /* Device memory the handle holds, in bytes (pair data, screening tables,
