@@ -275,7 +275,7 @@ def run_reference(args):
                       "e2e": {"value": v, "unit": "builds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
-LLDL_DRAM_BYTES_PER_QUARTET = 2811.0  # (130.4 + 3649.3 MB read + 37.9 MB written) / 5 builds / 271,664 quartets
+LLDL_DRAM_BYTES_PER_QUARTET = 2805.0  # (130.1 + 3647.0 MB read + 33.4 MB written) / 5 builds / 271,664 quartets
 
 
 def main():
