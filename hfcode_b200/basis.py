@@ -141,14 +141,19 @@ def read_basfile(path: str) -> Dict[str, ElementBasis]:
     return out
 
 
-def load_basis(name: str) -> Dict[str, ElementBasis]:
-    """Load one of the bundled basis files by name ('6-31G(d)', 'STO-3G')
-    or by path."""
+def basis_path(name: str) -> str:
+    """Path of a bundled basis file by name ('6-31G(d)', 'STO-3G'), or the
+    name itself when it is a path."""
     alias = {"6-31g(d)": "631Gd.dat", "631gd": "631Gd.dat", "6-31g*": "631Gd.dat",
              "sto-3g": "STO-3G.dat", "sto3g": "STO-3G.dat"}
     fn = alias.get(name.lower(), name)
-    path = fn if os.path.isabs(fn) or os.path.exists(fn) else os.path.join(DATA_DIR, fn)
-    return read_basfile(path)
+    return fn if os.path.isabs(fn) or os.path.exists(fn) else os.path.join(DATA_DIR, fn)
+
+
+def load_basis(name: str) -> Dict[str, ElementBasis]:
+    """Load one of the bundled basis files by name ('6-31G(d)', 'STO-3G')
+    or by path."""
+    return read_basfile(basis_path(name))
 
 
 @dataclasses.dataclass

@@ -17,6 +17,7 @@ import numpy as np
 
 from . import basis, fock
 from .basis import MAXPRIM, Molecule, ShellSet
+from .cabi import HfgpuBasis
 from .inputs import InputOptions
 
 EXPORTS = ["hfgpu_system_from_files", "hfgpu_system_from_atoms", "hfgpu_system_get_info",
@@ -67,20 +68,12 @@ class NativeSystem:
     nocc: int
 
 
-def _resolve(basfile: str) -> str:
-    alias = {"6-31g(d)": "631Gd.dat", "631gd": "631Gd.dat", "6-31g*": "631Gd.dat",
-             "sto-3g": "STO-3G.dat", "sto3g": "STO-3G.dat"}
-    import os
-    fn = alias.get(basfile.lower(), basfile)
-    return fn if os.path.isabs(fn) or os.path.exists(fn) else os.path.join(basis.DATA_DIR, fn)
-
-
 def load_system(basfile: str, infile: Optional[str] = None, labels: Optional[Sequence[str]] = None,
                 coords_ang: Optional[np.ndarray] = None) -> NativeSystem:
     """Read and lay out a system with the C++ input layer: either from a
     molecule input file or from element labels and Angstrom coordinates."""
     h = ctypes.c_void_p()
-    bas = _resolve(basfile).encode()
+    bas = basis.basis_path(basfile).encode()
     if infile is not None:
         _check(_lib.hfgpu_system_from_files(bas, infile.encode(), ctypes.byref(h)), "hfgpu_system_from_files")
     else:
@@ -91,7 +84,6 @@ def load_system(basfile: str, infile: Optional[str] = None, labels: Optional[Seq
     try:
         info = SystemInfo()
         _check(_lib.hfgpu_system_get_info(h, ctypes.byref(info)), "hfgpu_system_get_info")
-        from .cabi import HfgpuBasis
         v = HfgpuBasis()
         _check(_lib.hfgpu_system_basis(h, ctypes.byref(v)), "hfgpu_system_basis")
         nsh, nat = info.nsh, info.natom
