@@ -181,15 +181,19 @@ def mixed_study(fock, mol, sh, cutoffs, dev):
         DeviceSCF(wmol, wsh, fbw).run(basis.density_superposition(wmol, bas, wsh.nb), conve=1e-9, conv=1e-6,
                                       maxiter=80, fp32_cutoff=cut)
         fbw.close()
-    for label, cut in (("device_scf_fp64", 0.0), ("device_scf_mixed_1e-05", 1e-5)):
-        fbd = fock.FockBuilder(sh)
-        t1 = time.perf_counter()
-        rd = DeviceSCF(mol, sh, fbd, ints=ints).run(p0, conve=1e-9, conv=1e-6, maxiter=80, fp32_cutoff=cut)
-        sec = time.perf_counter() - t1
-        fbd.close()
-        out[label] = {"energy": rd.energy, "cycles": rd.cycles, "converged": rd.converged, "seconds": sec,
-                      "abs_dE_vs_host_fp64": abs(rd.energy - r64.energy),
-                      "scf_builds_per_s": rd.cycles / sec}
+    # the two forms alternate, twice each; the faster run of each is
+    # reported (these host-driven runs vary by tens of percent run to run)
+    for rep in range(2):
+        for label, cut in (("device_scf_fp64", 0.0), ("device_scf_mixed_1e-05", 1e-5)):
+            fbd = fock.FockBuilder(sh)
+            t1 = time.perf_counter()
+            rd = DeviceSCF(mol, sh, fbd, ints=ints).run(p0, conve=1e-9, conv=1e-6, maxiter=80, fp32_cutoff=cut)
+            sec = time.perf_counter() - t1
+            fbd.close()
+            runs = out.get(label, {}).get("runs_seconds", []) + [sec]
+            out[label] = {"energy": rd.energy, "cycles": rd.cycles, "converged": rd.converged, "seconds": min(runs),
+                          "runs_seconds": runs, "abs_dE_vs_host_fp64": abs(rd.energy - r64.energy),
+                          "scf_builds_per_s": rd.cycles / min(runs)}
     # a delta-P near convergence: the converged density against the core-free
     # one-cycle update (P_next - P), the size the incremental builds see late
     nb = sh.nb

@@ -154,3 +154,25 @@ def test_edge_densities_and_thresholds(case):
         assert st["pass"].sum() > 0
         assert np.max(np.abs(fg - fo)) < TOL
     fb.close()
+
+
+@pytest.mark.gpu
+def test_default_scratch_follows_the_molecule():
+    """The default scratch budget (24 GiB) is an upper bound: a handle
+    allocates only what its largest class list needs, so a small molecule's
+    device footprint stays small, and a tight explicit budget (more chunks)
+    gives the same F."""
+    from hfcode_b200.fock import FockBuilder
+    _, _, sh, p0 = system("benzene")
+    nb = sh.nb
+    out = []
+    for budget in (None, 1 << 20):
+        fb = FockBuilder(sh, scratch_budget=budget)
+        f = np.zeros((nb, nb))
+        fb.fock_build_initial_diag(f, p0, 1e-10)
+        fb.fock_build_non_diag(f, p0, 1e-10)
+        if budget is None:
+            assert fb.device_bytes() < (256 << 20)
+        out.append(f)
+        fb.close()
+    assert np.max(np.abs(out[0] - out[1])) < 1e-11
