@@ -376,9 +376,22 @@ def main():
     traffic = None
     if fock.CLASS_NAMES[top] == "LL|DL":
         traffic = LLDL_DRAM_BYTES_PER_QUARTET * float(st["pass"][top])
+    # the same class seen from HBM: its measured DRAM bytes per build over
+    # its time, against the measured copy bandwidth (fallback 6650 GB/s)
+    hbm_peak, hbm_src = 6650.0, "fallback 6650 GB/s (no MEASURED_PEAKS.json)"
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            hbm_peak, hbm_src = float(json.load(fh)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        pass
+    hbm_view = None
+    if traffic:
+        gbs = traffic / (st["ms"][top] * 1e-3) / 1e9
+        hbm_view = {"achieved": gbs, "peak": hbm_peak, "unit": "GB/s", "frac": gbs / hbm_peak,
+                    "peak_source": hbm_src}
     roof = {"bound": "fp64", "kernel": f"class {fock.CLASS_NAMES[top]} (role kernels + k_scatter_staged)",
             "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf,
-            "traffic": traffic, "traffic_unit": "bytes per build of the class",
+            "traffic": traffic, "traffic_unit": "bytes per build of the class", "hbm_view": hbm_view,
             "peak_source": "measured FP64 FMA-chain probe on this device (MEASURED_PEAKS.json has no FP64 figure)",
             "all_classes_tflops": float(cls_flops.sum() / (st["ms"].sum() * 1e-3) / 1e12),
             "class_ms": {fock.CLASS_NAMES[c]: round(float(st["ms"][c]), 3) for c in range(fock.NCLASS) if st["ms"][c] > 0},
