@@ -44,8 +44,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--molecule", default="c60")
-    ap.add_argument("--density", default="huckel", choices=["huckel", "guess"])
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--density", default="core_guess", choices=["core_guess", "atomic_guess"],
+                    help="core-Hamiltonian guess (dense, direct_hartreefock.f90:61-91) or the atomic-density "
+                         "guess (block-diagonal, :50-59)")
+    ap.add_argument("--cpu-stride", type=int, default=16,
+                    help="CPU legs: each step builds the bra rows ii %% stride == 0 of every class block")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the FP64-vs-mixed SCF study")
     ap.add_argument("--mixed-cutoffs", default="1e-7,1e-5,1e-3")
@@ -54,8 +57,12 @@ def parse():
     return ap.parse_args()
 
 
-def workload(name: str, density: str):
-    from hfcode_b200 import basis, molecules, onee
+def workload(name: str, density: str, oracle_side: bool = False):
+    """Molecule, shells and the fixed density of one bench step.  The core
+    guess needs S, T, V: the GPU arm takes them from this library, the CPU
+    reference arm from the oracle (oracle/oscf.py), so that arm never loads
+    libhfgpu.so; both give the same density to rounding."""
+    from hfcode_b200 import basis, molecules
     if name == "c60":
         mol, bas = molecules.c60(), basis.load_basis("6-31G(d)")
         label = "C60/6-31G(d)"
@@ -67,11 +74,22 @@ def workload(name: str, density: str):
         mol, bas = molecules.alkane(n), basis.load_basis("6-31G(d)")
         label = f"C{n}H{2 * n + 2}/6-31G(d)"
     sh = basis.spread_basis(mol, bas)
-    if density == "guess":
+    if density == "atomic_guess":
         p = basis.density_superposition(mol, bas, sh.nb)
+    elif oracle_side:
+        from oracle import oscf
+        p = oscf.OracleSCF(mol.charges, mol.coords, mol.nocc, sh).core_density()
     else:
-        p = onee.huckel_density(mol, sh)
+        from hfcode_b200 import onee
+        p = onee.core_density(mol, sh)
     return label, mol, sh, p
+
+
+def bench_config(label: str, nb: int, density: str, world: int) -> dict:
+    """The workload description, identical in the GPU arm and the reference arm."""
+    return {"workload": f"{label} one Fock build (fock_build_diag + fock_build_non_diag), thr=1e-10",
+            "nb": nb, "density": density, "parallelism": f"replicas{world}",
+            "l2": "GPU arm: flushed between steps (256 MiB write outside the timed events)"}
 
 
 class ClockSampler:
@@ -125,30 +143,44 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(sh, p, target_s: float, n_pass_total: int):
-    """Oracle (reference restatement) on the host cores, bounded row sample."""
+def cpu_oracle_builds(sh, p, warmup: int, steps: int, stride: int, calibrate: bool = True) -> dict:
+    """The oracle (a C++/OpenMP restatement of the reference's builders) on
+    all host cores.  Each step is fock_build_diag in full plus
+    fock_build_non_diag on the same fixed rows every step: the bra rows
+    ii % stride == 0 of every class block (the rows are in descending Schwarz
+    order, so this is a stratified 1/stride sample).  One unsampled
+    fock_build_non_diag, timed once after the steps, calibrates the
+    extrapolation: ratio = t_full / (stride * t_sample)."""
     from oracle import pyoracle
     orc = pyoracle.Oracle(sh)
     nb = sh.nb
     f = np.zeros((nb, nb))
     orc.fock_build_initial_diag(f, p, THR)
-    t0 = time.perf_counter()
-    orc.fock_build_diag(f, p, THR)
-    t_diag = time.perf_counter() - t0
-    stride = 4096
-    while True:
+    td, ts = [], []
+    for it in range(warmup + steps):
         t0 = time.perf_counter()
+        orc.fock_build_diag(f, p, THR)
+        t1 = time.perf_counter()
         n = orc.fock_build_non_diag_sample(f, p, THR, stride, 0)
-        dt = time.perf_counter() - t0
-        if dt > 0.3 * target_s or stride == 1:
-            break
-        stride = max(1, int(stride * max(0.05, dt) / target_s))
-    t_full = t_diag + dt * (n_pass_total / max(n, 1))
+        t2 = time.perf_counter()
+        if it >= warmup:
+            td.append(t1 - t0)
+            ts.append(t2 - t1)
+    t_diag, t_samp = float(np.median(td)), float(np.median(ts))
+    cal = {"ratio": 1.0, "full_non_diag_s": None}
+    if calibrate:
+        t0 = time.perf_counter()
+        orc.fock_build_non_diag(f, p, THR)
+        t_full = time.perf_counter() - t0
+        cal = {"ratio": t_full / (stride * t_samp), "full_non_diag_s": t_full,
+               "sampled_non_diag_s": t_samp, "stride": stride}
+    t_build = t_diag + stride * t_samp * cal["ratio"]
     threads = pyoracle.lib().orc_num_threads()
-    return {"value": 1.0 / t_full, "unit": "builds/s", "cores": threads, "kind": "port",
-            "sample": f"bra rows ii % {stride} == 0 of every class block: {n} of {n_pass_total} screened-in "
-                      f"quartets in {dt:.1f} s, extrapolated by quartet count; diag part timed in full "
-                      f"({t_diag:.2f} s)"}
+    return {"value": 1.0 / t_build, "unit": "builds/s", "cores": threads, "kind": "port", "extrapolated": True,
+            "step_seconds": t_diag + t_samp, "calibration": cal,
+            "sample": f"each step: fock_build_diag in full + fock_build_non_diag on the fixed bra rows ii % {stride} "
+                      f"== 0 of every class block ({n} screened-in quartets); extrapolated x{stride} times the "
+                      f"calibration ratio of one unsampled build in the same run"}
 
 
 def mixed_study(fock, mol, sh, cutoffs, dev):
@@ -242,39 +274,21 @@ def mixed_study(fock, mol, sh, cutoffs, dev):
 
 
 def run_reference(args):
+    """The reference arm: the oracle on the host cores for the same workload,
+    density and metric.  It loads only oracle/liboracle.so (the density comes
+    from the oracle's own one-electron integrals)."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    label, mol, sh, p = workload(args.molecule, args.density)
-    # the screened-in quartet count of the full build, from the oracle's own
-    # screen on a full pass of the cheap diag + count-only sample scale
-    from oracle import pyoracle
-    orc = pyoracle.Oracle(sh)
-    f = np.zeros((sh.nb, sh.nb))
-    orc.fock_build_initial_diag(f, p, THR)
-    vals = []
-    samples = []
-    for it in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        orc.fock_build_diag(f, p, THR)
-        td = time.perf_counter() - t0
-        stride = max(1, int(os.environ.get("HF_REF_STRIDE", "64")))
-        t0 = time.perf_counter()
-        n = orc.fock_build_non_diag_sample(f, p, THR, stride, it % stride)
-        ts = time.perf_counter() - t0
-        if it >= args.warmup:
-            vals.append(1.0 / (td + ts * stride))
-            samples.append(n)
-    v = float(np.median(vals))
-    threads = pyoracle.lib().orc_num_threads()
-    cb = {"value": v, "unit": "builds/s", "cores": threads, "kind": "port",
-          "sample": f"each step: fock_build_diag in full + fock_build_non_diag on bra rows ii % {stride} == step "
-                    f"(~1/{stride} of the quartets), time x{stride}"}
+    label, mol, sh, p = workload(args.molecule, args.density, oracle_side=True)
+    cb = cpu_oracle_builds(sh, p, args.warmup, args.steps, args.cpu_stride, calibrate=True)
+    v = cb["value"]
     print(json.dumps({"metric": METRIC, "value": v, "unit": "builds/s", "impl": "reference", "n_gpus": 0,
-                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v,
-                      "higher_is_better": True, "dtype": "f64", "data": "synthetic",
-                      "config": {"workload": f"{label} one Fock build (diag + non_diag), thr=1e-10",
-                                 "nb": sh.nb, "density": args.density},
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * cb["step_seconds"],
+                      "ms_per_step_note": "wall time of one sampled step (the value is extrapolated from it)",
+                      "extrapolated": True, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+                      "config": bench_config(label, sh.nb, args.density, world),
                       "cpu_baseline": cb,
                       "e2e": {"value": v, "unit": "builds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
@@ -403,9 +417,7 @@ def main():
            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None,
            "dtype": "f64" if args.cutoff <= 0 else f"f64 + f32 below bound {args.cutoff:g}", "data": "synthetic",
-           "config": {"workload": f"{label} one Fock build (fock_build_diag + fock_build_non_diag), thr=1e-10",
-                      "nb": nb, "density": args.density, "parallelism": f"replicas{world}",
-                      "l2": "flushed between steps (256 MiB write outside the timed events)"},
+           "config": bench_config(label, nb, args.density, world),
            "quartets_per_s": n_pass * value, "screened_in_quartets": n_pass,
            "e2e": e2e, "gpu_launches": n_launch, "roofline": roof,
            "fp64_peak_tflops": peak_tf, "fp32_peak_tflops": fp32_peak / 1e3,
@@ -413,7 +425,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_mixed:
         out["mixed"] = mixed_study(fock, mol, sh, [float(x) for x in args.mixed_cutoffs.split(",")], dev)
     if rank == 0 and world == 1 and not args.no_cpu:
-        out["cpu_baseline"] = cpu_baseline(sh, p, args.cpu_seconds, n_pass)
+        out["cpu_baseline"] = cpu_oracle_builds(sh, p, 1, 2, args.cpu_stride, calibrate=True)
     if rank == 0:
         print(json.dumps(out))
     fb.close()

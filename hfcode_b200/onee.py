@@ -54,8 +54,3 @@ def core_density(mol: Molecule, sh: ShellSet, ints=None) -> np.ndarray:
     C = X @ C
     occ = C[:, :mol.nocc]
     return 2.0 * occ @ occ.T
-
-
-def huckel_density(mol: Molecule, sh: ShellSet) -> np.ndarray:
-    """Dense benchmark density: the core-Hamiltonian guess."""
-    return core_density(mol, sh)

@@ -47,6 +47,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <numeric>
 #include <tuple>
@@ -198,18 +199,19 @@ const Cart* carts(int t) {
 // matharmond (index_functions.f90:158-167): spherical d (z2,xz,yz,xy,x2-y2)
 // from Cartesian (xx,xy,xz,yy,yz,zz)
 double harm(int s, int c) {
-    static double M[5][6];
-    static bool init = false;
-    if (!init) {
-        std::memset(M, 0, sizeof(M));
-        M[0][5] = 1.0; M[0][0] = -.5; M[0][3] = -.5;
-        M[1][2] = std::sqrt(3.0);
-        M[2][4] = std::sqrt(3.0);
-        M[3][1] = std::sqrt(3.0);
-        M[4][0] = std::sqrt(3.0) / 2.0; M[4][3] = -std::sqrt(3.0) / 2.0;
-        init = true;
-    }
-    return M[s][c];
+    struct Tab {
+        double M[5][6];
+        Tab() {
+            std::memset(M, 0, sizeof(M));
+            M[0][5] = 1.0; M[0][0] = -.5; M[0][3] = -.5;
+            M[1][2] = std::sqrt(3.0);
+            M[2][4] = std::sqrt(3.0);
+            M[3][1] = std::sqrt(3.0);
+            M[4][0] = std::sqrt(3.0) / 2.0; M[4][3] = -std::sqrt(3.0) / 2.0;
+        }
+    };
+    static const Tab tab;  // initialised once, thread-safe
+    return tab.M[s][c];
 }
 
 /* ---------------- 4-centre Obara-Saika plan ---------------------------- */
@@ -225,6 +227,7 @@ struct Plan {
     std::vector<Op> ops;
     std::vector<Term> terms;
     std::vector<int> target;  // op index per cartesian (a,b,c,d) target
+    std::vector<uint8_t> wpat;  // per target: bit c set when centre c's component is an L-shell p
 };
 
 struct Key {
@@ -336,8 +339,24 @@ struct Oracle {
             }
             key4.m = 0;
             b.plan.target.push_back(b.get(key4));
+            const int ts[4] = {t1, t2, t3, t4};
+            uint8_t pat = 0;
+            for (int c = 0; c < 4; ++c)
+                if (ts[c] == HFGPU_SHELL_L && (cs[c]->x + cs[c]->y + cs[c]->z) == 1) pat |= (uint8_t)(1 << c);
+            b.plan.wpat.push_back(pat);
         }
-        return plans.emplace(key, std::move(b.plan)).first->second;
+        const Plan& pl = plans.emplace(key, std::move(b.plan)).first->second;
+        fast[tix(t1)][tix(t2)][tix(t3)][tix(t4)] = &pl;
+        return pl;
+    }
+
+    // Plans by shell-type index (S P D L -> 0..3), filled by plan_for; the
+    // OpenMP regions only read this table (init builds every plan they use).
+    const Plan* fast[4][4][4][4] = {};
+    static int tix(int t) { return t == HFGPU_SHELL_S ? 0 : t == HFGPU_SHELL_P ? 1 : t == HFGPU_SHELL_D ? 2 : 3; }
+    const Plan& plan_fast(int t1, int t2, int t3, int t4) {
+        const Plan* p = fast[tix(t1)][tix(t2)][tix(t3)][tix(t4)];
+        return p ? *p : plan_for(t1, t2, t3, t4);
     }
 
     int classof(int ta, int tb) const {
@@ -409,24 +428,22 @@ struct Oracle {
     }
 
     // Contracted ERI block of (s1 s2|s3 s4) over the pairs' stored prims.
-    // out[((i*n2+j)*n3+k)*n4+l] in each shell's function order.
+    // out[((i*n2+j)*n3+k)*n4+l] in each shell's function order.  The plan,
+    // its per-target L-weight pattern and every work array are looked up or
+    // reused, so a call allocates nothing once its thread has run one quartet.
     void eri(int pab, int pcd, double* out) {
         const PairData& A = pairs[pab];
         const PairData& C = pairs[pcd];
         int s[4] = {A.sh1, A.sh2, C.sh1, C.sh2};
         int t[4] = {shtyp[s[0]], shtyp[s[1]], shtyp[s[2]], shtyp[s[3]]};
-        const Plan& pl = plan_for(t[0], t[1], t[2], t[3]);
+        const Plan& pl = plan_fast(t[0], t[1], t[2], t[3]);
         int nc[4] = {ncart(t[0]), ncart(t[1]), ncart(t[2]), ncart(t[3])};
         int ncart4 = nc[0] * nc[1] * nc[2] * nc[3];
         int L = lmax(t[0]) + lmax(t[1]) + lmax(t[2]) + lmax(t[3]);
-        std::vector<double> acc(ncart4, 0.0), v(pl.ops.size());
+        thread_local std::vector<double> acc, v, cur, nx;
+        acc.assign(ncart4, 0.0);
+        if (v.size() < pl.ops.size()) v.resize(pl.ops.size());
         const double* X[4] = {&xsh[3 * s[0]], &xsh[3 * s[1]], &xsh[3 * s[2]], &xsh[3 * s[3]]};
-        // per-component weights: p components of L shells carry the djkl ratio
-        std::vector<int> isp[4];
-        for (int c = 0; c < 4; ++c) {
-            const Cart* cc = carts(t[c]);
-            for (int i = 0; i < nc[c]; ++i) isp[c].push_back(t[c] == HFGPU_SHELL_L && (cc[i].x + cc[i].y + cc[i].z) == 1);
-        }
         double fm[32];
         double cf[C_NCOEF];
         for (const PrimPair& pa : A.prims) {
@@ -453,41 +470,44 @@ struct Oracle {
                 cf[C_H2Q] = 0.5 / q;
                 cf[C_RH2Q] = -0.5 / q * (rho / q);
                 cf[C_H2PQ] = 0.5 * ooppq;
-                for (size_t o = 0; o < pl.ops.size(); ++o) {
+                const size_t nops = pl.ops.size();
+                for (size_t o = 0; o < nops; ++o) {
                     const Op& op = pl.ops[o];
                     if (op.nterm == 0) { v[o] = pref * fm[op.m]; continue; }
-                    double s = 0;
-                    for (int tt = 0; tt < op.nterm; ++tt) {
-                        const Term& tm = pl.terms[op.first + tt];
-                        s += cf[tm.coef] * tm.mult * v[tm.child];
-                    }
-                    v[o] = s;
+                    double sum = 0;
+                    const Term* tm = &pl.terms[op.first];
+                    for (int tt = 0; tt < op.nterm; ++tt) sum += cf[tm[tt].coef] * tm[tt].mult * v[tm[tt].child];
+                    v[o] = sum;
                 }
-                // weights of L-shell p components (s_d_l_terms.f90:1885-1896)
-                double w[4][2];
-                w[0][0] = w[1][0] = w[2][0] = w[3][0] = 1.0;
-                w[0][1] = djkl[(size_t)s[0] * maxprim + pa.za];
-                w[1][1] = djkl[(size_t)s[1] * maxprim + pa.zb];
-                w[2][1] = djkl[(size_t)s[2] * maxprim + pc.za];
-                w[3][1] = djkl[(size_t)s[3] * maxprim + pc.zb];
-                int n = 0;
-                for (int i = 0; i < nc[0]; ++i) for (int j = 0; j < nc[1]; ++j)
-                for (int k = 0; k < nc[2]; ++k) for (int l = 0; l < nc[3]; ++l, ++n) {
-                    double ww = w[0][isp[0][i]] * w[1][isp[1][j]] * w[2][isp[2][k]] * w[3][isp[3][l]];
-                    acc[n] += ww * v[pl.target[n]];
+                // weights of L-shell p components (s_d_l_terms.f90:1885-1896):
+                // wt[pattern] for the 16 patterns of p-component centres
+                double w[4];
+                w[0] = djkl[(size_t)s[0] * maxprim + pa.za];
+                w[1] = djkl[(size_t)s[1] * maxprim + pa.zb];
+                w[2] = djkl[(size_t)s[2] * maxprim + pc.za];
+                w[3] = djkl[(size_t)s[3] * maxprim + pc.zb];
+                double wt[16];
+                for (int m = 0; m < 16; ++m) {
+                    double x = 1.0;
+                    for (int c = 0; c < 4; ++c)
+                        if (m & (1 << c)) x *= w[c];
+                    wt[m] = x;
                 }
+                const int* tg = pl.target.data();
+                const uint8_t* wp = pl.wpat.data();
+                for (int n = 0; n < ncart4; ++n) acc[n] += wt[wp[n]] * v[tg[n]];
             }
         }
         // Cartesian -> spherical for d shells
         int nf[4] = {nfunc(t[0]), nfunc(t[1]), nfunc(t[2]), nfunc(t[3])};
-        std::vector<double> cur = acc;
+        cur.assign(acc.begin(), acc.end());
         int dims[4] = {nc[0], nc[1], nc[2], nc[3]};
         for (int c = 0; c < 4; ++c) {
             if (t[c] != HFGPU_SHELL_D) continue;
             int outer = 1, inner = 1;
             for (int q = 0; q < c; ++q) outer *= dims[q];
             for (int q = c + 1; q < 4; ++q) inner *= dims[q];
-            std::vector<double> nx((size_t)outer * 5 * inner, 0.0);
+            nx.assign((size_t)outer * 5 * inner, 0.0);
             for (int o = 0; o < outer; ++o)
                 for (int sidx = 0; sidx < 5; ++sidx)
                     for (int cc = 0; cc < 6; ++cc) {
@@ -501,6 +521,183 @@ struct Oracle {
         }
         int nout = nf[0] * nf[1] * nf[2] * nf[3];
         std::memcpy(out, cur.data(), sizeof(double) * nout);
+    }
+
+    // One-electron integrals S, T, V (cmpt1e.f90 with one_electron_terms.f90:
+    // s_s_1e_terms ... d_l_1e_terms): every primitive pair of every shell
+    // pair (no negab screen there), coefficients djk_a*djk_b with the L-shell
+    // p/s ratio djkl on p components, the Boys routine of the pair's total
+    // angular momentum (boys_0/1/2/n as each *_1e_terms routine calls it),
+    // Cartesian d transformed with matharmond.  Obara-Saika recurrences:
+    //   overlap    s(i+1,j) = PA s(i,j) + (i s(i-1,j) + j s(i,j-1))/2p, per axis
+    //   kinetic    t(i,j) = -2b^2 s(i,j+2) + b(2j+1) s(i,j) - j(j-1)/2 s(i,j-2)
+    //   nuclear    V(a+1,b)^m = PA V(a,b)^m - PC V(a,b)^(m+1)
+    //                          + a/2p (V(a-1,b)^m - V(a-1,b)^(m+1)) + b/2p (...)
+    //              V(0,0)^m = 2 pi/p exp(-ab/p AB^2) F_m(p PC^2)
+    // S, T, V are nb x nb, symmetric, written in full.
+    void one_electron(int natom, const double* Z, const double* xyz, double* S, double* T, double* V) {
+        const size_t nb2 = (size_t)nb * nb;
+        std::fill(S, S + nb2, 0.0);
+        std::fill(T, T + nb2, 0.0);
+        std::fill(V, V + nb2, 0.0);
+        std::vector<std::pair<int, int>> plist;
+        for (int a = 0; a < nsh; ++a)
+            for (int b = 0; b <= a; ++b) plist.push_back({a, b});
+#pragma omp parallel for schedule(dynamic)
+        for (long long ip = 0; ip < (long long)plist.size(); ++ip) {
+            const int a = plist[ip].first, b = plist[ip].second;
+            const int ta = shtyp[a], tb = shtyp[b];
+            const int na = ncart(ta), nbc = ncart(tb);
+            const Cart* ca = carts(ta);
+            const Cart* cb = carts(tb);
+            const int la = lmax(ta), lb = lmax(tb), nboys = la + lb;
+            double cs[6][6] = {}, ct[6][6] = {}, cv[6][6] = {};
+            const double* A = &xsh[3 * a];
+            const double* B = &xsh[3 * b];
+            double ab2 = 0;
+            for (int x = 0; x < 3; ++x) ab2 += (A[x] - B[x]) * (A[x] - B[x]);
+            for (int za = 0; za < nzet[a]; ++za)
+                for (int zb = 0; zb < nzet[b]; ++zb) {
+                    const double ea = zeta[(size_t)a * maxprim + za], eb = zeta[(size_t)b * maxprim + zb];
+                    const double p = ea + eb, op = 1.0 / p, mu = ea * eb * op;
+                    const double dd = djk[(size_t)a * maxprim + za] * djk[(size_t)b * maxprim + zb];
+                    const double ga = djkl[(size_t)a * maxprim + za], gb = djkl[(size_t)b * maxprim + zb];
+                    const double K = std::exp(-mu * ab2);
+                    double P[3], PA[3], PB[3];
+                    for (int x = 0; x < 3; ++x) {
+                        P[x] = (ea * A[x] + eb * B[x]) * op;
+                        PA[x] = P[x] - A[x];
+                        PB[x] = P[x] - B[x];
+                    }
+                    // 1D overlap tables s[x][i][j], i <= la, j <= lb + 2
+                    double s1[3][3][5];
+                    for (int x = 0; x < 3; ++x) {
+                        for (int i = 0; i < 3; ++i)
+                            for (int j = 0; j < 5; ++j) s1[x][i][j] = 0.0;
+                        s1[x][0][0] = 1.0;
+                        for (int j = 0; j < 4; ++j)
+                            s1[x][0][j + 1] = PB[x] * s1[x][0][j] + (j > 0 ? 0.5 * op * j * s1[x][0][j - 1] : 0.0);
+                        for (int i = 0; i < 2; ++i)
+                            for (int j = 0; j < 5; ++j) {
+                                double v = PA[x] * s1[x][i][j];
+                                if (i > 0) v += 0.5 * op * i * s1[x][i - 1][j];
+                                if (j > 0) v += 0.5 * op * j * s1[x][i][j - 1];
+                                s1[x][i + 1][j] = v;
+                            }
+                    }
+                    const double s00 = std::pow(PI * op, 1.5) * K;
+                    auto t1 = [&](int x, int i, int j) {
+                        double v = -2.0 * eb * eb * s1[x][i][j + 2] + eb * (2 * j + 1) * s1[x][i][j];
+                        if (j >= 2) v -= 0.5 * j * (j - 1) * s1[x][i][j - 2];
+                        return v;
+                    };
+                    // nuclear attraction: V[a][b][m] over Cartesian exponents
+                    // (la, lb <= 2 -> exponent vectors indexed 0..26)
+                    double vn[6][6] = {};
+                    for (int nuc = 0; nuc < natom; ++nuc) {
+                        double PC[3], pc2 = 0;
+                        for (int x = 0; x < 3; ++x) {
+                            PC[x] = P[x] - xyz[3 * nuc + x];
+                            pc2 += PC[x] * PC[x];
+                        }
+                        double fm[16];
+                        boys(nboys, p * pc2, fm);
+                        // memo[ia][ib][m], ia/ib = exponent index ex*9+ey*3+ez
+                        const double base = 2.0 * PI * op * K;
+                        std::function<double(int, int, int, int, int, int, int)> rec;
+                        double memo[27][27][5];
+                        bool done[27][27][5] = {};
+                        rec = [&](int ax, int ay, int az, int bx, int by, int bz, int m) -> double {
+                            if (ax < 0 || ay < 0 || az < 0 || bx < 0 || by < 0 || bz < 0) return 0.0;
+                            const int ia = ax * 9 + ay * 3 + az, ib = bx * 9 + by * 3 + bz;
+                            if (done[ia][ib][m]) return memo[ia][ib][m];
+                            double r;
+                            int av[3] = {ax, ay, az}, bv[3] = {bx, by, bz};
+                            if (ax + ay + az > 0) {
+                                int i = ax > 0 ? 0 : ay > 0 ? 1 : 2;
+                                av[i] -= 1;
+                                r = PA[i] * rec(av[0], av[1], av[2], bx, by, bz, m) -
+                                    PC[i] * rec(av[0], av[1], av[2], bx, by, bz, m + 1);
+                                if (av[i] > 0) {
+                                    int a2[3] = {av[0], av[1], av[2]};
+                                    a2[i] -= 1;
+                                    r += 0.5 * op * av[i] *
+                                         (rec(a2[0], a2[1], a2[2], bx, by, bz, m) - rec(a2[0], a2[1], a2[2], bx, by, bz, m + 1));
+                                }
+                                if (bv[i] > 0) {
+                                    int b2[3] = {bx, by, bz};
+                                    b2[i] -= 1;
+                                    r += 0.5 * op * bv[i] *
+                                         (rec(av[0], av[1], av[2], b2[0], b2[1], b2[2], m) -
+                                          rec(av[0], av[1], av[2], b2[0], b2[1], b2[2], m + 1));
+                                }
+                            } else if (bx + by + bz > 0) {
+                                int i = bx > 0 ? 0 : by > 0 ? 1 : 2;
+                                bv[i] -= 1;
+                                r = PB[i] * rec(0, 0, 0, bv[0], bv[1], bv[2], m) -
+                                    PC[i] * rec(0, 0, 0, bv[0], bv[1], bv[2], m + 1);
+                                if (bv[i] > 0) {
+                                    int b2[3] = {bv[0], bv[1], bv[2]};
+                                    b2[i] -= 1;
+                                    r += 0.5 * op * bv[i] *
+                                         (rec(0, 0, 0, b2[0], b2[1], b2[2], m) - rec(0, 0, 0, b2[0], b2[1], b2[2], m + 1));
+                                }
+                            } else {
+                                r = base * fm[m];
+                            }
+                            done[ia][ib][m] = true;
+                            memo[ia][ib][m] = r;
+                            return r;
+                        };
+                        for (int i = 0; i < na; ++i)
+                            for (int j = 0; j < nbc; ++j)
+                                vn[i][j] -= Z[nuc] * rec(ca[i].x, ca[i].y, ca[i].z, cb[j].x, cb[j].y, cb[j].z, 0);
+                    }
+                    for (int i = 0; i < na; ++i)
+                        for (int j = 0; j < nbc; ++j) {
+                            double w = dd;
+                            if (ta == HFGPU_SHELL_L && ca[i].x + ca[i].y + ca[i].z == 1) w *= ga;
+                            if (tb == HFGPU_SHELL_L && cb[j].x + cb[j].y + cb[j].z == 1) w *= gb;
+                            const int ix = ca[i].x, iy = ca[i].y, iz = ca[i].z;
+                            const int jx = cb[j].x, jy = cb[j].y, jz = cb[j].z;
+                            const double sx = s1[0][ix][jx], sy = s1[1][iy][jy], sz = s1[2][iz][jz];
+                            cs[i][j] += w * s00 * sx * sy * sz;
+                            ct[i][j] += w * s00 * (t1(0, ix, jx) * sy * sz + sx * t1(1, iy, jy) * sz + sx * sy * t1(2, iz, jz));
+                            cv[i][j] += w * vn[i][j];
+                        }
+                }
+            // Cartesian -> spherical d (matharmond) on each d side
+            const int fa = nfunc(ta), fb = nfunc(tb);
+            double* mats[3] = {&cs[0][0], &ct[0][0], &cv[0][0]};
+            double* outs[3] = {S, T, V};
+            for (int k = 0; k < 3; ++k) {
+                double (*m)[6] = (double (*)[6])mats[k];
+                double r1[6][6] = {};
+                for (int i = 0; i < fa; ++i)
+                    for (int j = 0; j < nbc; ++j) {
+                        if (ta == HFGPU_SHELL_D) {
+                            double x = 0;
+                            for (int c = 0; c < 6; ++c) x += harm(i, c) * m[c][j];
+                            r1[i][j] = x;
+                        } else {
+                            r1[i][j] = m[i][j];
+                        }
+                    }
+                for (int i = 0; i < fa; ++i)
+                    for (int j = 0; j < fb; ++j) {
+                        double x;
+                        if (tb == HFGPU_SHELL_D) {
+                            x = 0;
+                            for (int c = 0; c < 6; ++c) x += harm(j, c) * r1[i][c];
+                        } else {
+                            x = r1[i][j];
+                        }
+                        const size_t r = (size_t)aosh[a] + i, c = (size_t)aosh[b] + j;
+                        outs[k][c * nb + r] = x;
+                        outs[k][r * nb + c] = x;
+                    }
+            }
+        }
     }
 
     int nfunc_pair(int pid) const { return nfunc(shtyp[pairs[pid].sh1]) * nfunc(shtyp[pairs[pid].sh2]); }
@@ -778,6 +975,12 @@ void orc_maxdm(void* h, const double* p, double* md_sh) {
     for (int a = 0; a < o->nsh; ++a)
         for (int b = 0; b < o->nsh; ++b)
             md_sh[(size_t)a * o->nsh + b] = md[o->pairid[(size_t)a * o->nsh + b]];
+}
+
+// One-electron integrals S, T, V (nb x nb, symmetric) for natom nuclei of
+// charges Z at xyz (bohr, row per atom).
+void orc_one_electron(void* h, int natom, const double* Z, const double* xyz, double* S, double* T, double* V) {
+    ((Oracle*)h)->one_electron(natom, Z, xyz, S, T, V);
 }
 
 int orc_num_threads() {

@@ -44,6 +44,7 @@ def _lib():
     lib.orc_counts.argtypes = [vp, ll, ll]
     lib.orc_maxdm.argtypes = [vp, d, d]
     lib.orc_num_threads.restype = ctypes.c_int
+    lib.orc_one_electron.argtypes = [vp, ctypes.c_int, d, d, d, d, d]
     lib.orc_fock_build_non_diag_sample.argtypes = [vp, d, d, ctypes.c_double, ctypes.c_int, ctypes.c_int]
     lib.orc_fock_build_non_diag_sample.restype = ctypes.c_longlong
     return lib
@@ -134,6 +135,14 @@ class Oracle:
         b = (ctypes.c_longlong * 100)()
         lib().orc_counts(self.h, a, b)
         return np.array(list(a)).reshape(10, 10), np.array(list(b)).reshape(10, 10)
+
+    def one_electron(self, charges, coords):
+        """S, T, V (nb x nb) for nuclei of the given charges at coords (bohr)."""
+        z = np.ascontiguousarray(charges, dtype=np.float64)
+        x = np.ascontiguousarray(coords, dtype=np.float64).reshape(-1, 3)
+        S, T, V = (np.zeros((self.nb, self.nb)) for _ in range(3))
+        lib().orc_one_electron(self.h, len(z), _dp(z), _dp(x), _dp(S), _dp(T), _dp(V))
+        return S, T, V
 
     def maxdm(self, p):
         out = np.zeros((self.nsh, self.nsh))

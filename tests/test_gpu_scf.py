@@ -51,14 +51,16 @@ def test_pure_p_basis_energy(name):
 @pytest.mark.parametrize("name", ["h2", "ne"])
 def test_gpu_scf_small_edge_systems(name):
     """Two s shells only (H2) and one centre (Ne: every quartet has
-    AB = CD = PQ = 0): the GPU SCF energy against the oracle's SCF, computed
-    here (both small), to 1e-8 Eh."""
+    AB = CD = PQ = 0): the GPU SCF energy against the oracle's own SCF
+    (oracle/oscf.py: oracle integrals and protocol), computed here (both
+    small), to 1e-8 Eh."""
     from hfcode_b200.fock import FockBuilder
-    from oracle import pyoracle
+    from oracle import oscf
     mol, _, sh, p0 = system(name)
-    ref = scf.direct_hartreefock(mol, sh, pyoracle.Oracle(sh), p_guess=p0, conve=1e-10, conv=1e-7, maxiter=60)
+    ref = oscf.OracleSCF(mol.charges, mol.coords, mol.nocc, sh).run(p_guess=p0, conve=1e-10, conv=1e-7,
+                                                                     maxiter=60)
     fb = FockBuilder(sh)
     r = scf.direct_hartreefock(mol, sh, fb, p_guess=p0, conve=1e-10, conv=1e-7, maxiter=60)
     fb.close()
-    assert r.converged and ref.converged
-    assert abs(r.energy - ref.energy) < ETOL, (r.energy, ref.energy)
+    assert r.converged and ref["converged"]
+    assert abs(r.energy - ref["energy"]) < ETOL, (r.energy, ref["energy"])

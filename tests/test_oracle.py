@@ -124,3 +124,42 @@ def test_maxdm_dl_block_follows_reference():
     P[sh.aosh[d], sh.aosh[l1] + 4] = P[sh.aosh[l1] + 4, sh.aosh[d]] = 3.0   # function after l: read
     md = orc.maxdm(P)
     assert md[d, l1] == 3.0
+
+
+@pytest.mark.parametrize("name", ["water", "alkane2_mix", "benzene"])
+def test_oracle_one_electron_matches_mcmurchie_davidson(name):
+    """The oracle's own S, T, V (cmpt1e.f90 / one_electron_terms.f90
+    restated) against the independent McMurchie-Davidson evaluation on
+    sampled shell pairs of every type combination present."""
+    import mdref
+    mol, _, sh, _ = system(name)
+    S, T, V = pyoracle.Oracle(sh).one_electron(mol.charges, mol.coords)
+    assert np.max(np.abs(S - S.T)) == 0 and np.max(np.abs(V - V.T)) == 0
+    atoms = list(zip(mol.charges, mol.coords))
+    nfunc = {1: 1, 2: 3, 3: 5, 12: 4}
+    by_kind = {}
+    for a in range(sh.nsh):
+        for b in range(a + 1):
+            by_kind.setdefault((int(sh.shtyp[a]), int(sh.shtyp[b]), a == b), []).append((a, b))
+    rng = np.random.default_rng(7)
+    for lst in by_kind.values():
+        for k in rng.choice(len(lst), size=min(2, len(lst)), replace=False):
+            a, b = lst[k]
+            ref = mdref.shell_onee(sh, a, b, atoms)
+            oa, ob = int(sh.aosh[a]), int(sh.aosh[b])
+            na, nb = nfunc[int(sh.shtyp[a])], nfunc[int(sh.shtyp[b])]
+            for got, r in zip((S, T, V), ref):
+                blk = got[oa:oa + na, ob:ob + nb]
+                assert np.max(np.abs(blk - r)) < 1e-10 * max(1.0, np.max(np.abs(r))), (name, a, b)
+
+
+def test_oracle_scf_protocol_matches_golden():
+    """The oracle's SCF (oracle/oscf.py) reproduces the golden water energy,
+    which make_golden.py wrote with it (regression of the protocol)."""
+    import json
+    import os
+    from oracle import oscf
+    gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "energies.json")))["water"]
+    mol, _, sh, p0 = system("water")
+    r = oscf.OracleSCF(mol.charges, mol.coords, mol.nocc, sh).run(p_guess=p0, conve=1e-10, conv=1e-7)
+    assert r["converged"] and abs(r["energy"] - gold["energy"]) < 1e-9
