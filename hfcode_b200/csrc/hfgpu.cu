@@ -294,6 +294,7 @@ struct hfgpu_handle {
     std::vector<int> last_ref;            // lastXX per reference class
     bool have_schwarz = false;
     int timing = 0;
+    int no_fused = 0;                     // 1: fused classes take the staged path (A/B comparisons)
     cudaStream_t stream = nullptr;
     cudaStream_t aux[NSTREAM] = {};    // independent classes run concurrently on these
     cudaEvent_t fork = nullptr, join[NSTREAM] = {};
@@ -402,6 +403,8 @@ struct ClassTable {
                 cudaFuncSetAttribute(k[c].scat, cudaFuncAttributeMaxDynamicSharedMemorySize, k[c].scat_smem);
             if (k[c].scat32 && k[c].scat32_smem > 0)
                 cudaFuncSetAttribute(k[c].scat32, cudaFuncAttributeMaxDynamicSharedMemorySize, k[c].scat32_smem);
+            if (k[c].fz64 && k[c].fz_smem > 0)
+                cudaFuncSetAttribute(k[c].fz64, cudaFuncAttributeMaxDynamicSharedMemorySize, k[c].fz_smem);
         }
     }
 };
@@ -729,9 +732,43 @@ int build_active(hfgpu_handle* h) {
 
 // Staged class: chunks of the quartet list through the accumulator roles
 // (mode 2), the output roles and the scatter kernel.
+// Fused class (FP64 quartets): one launch over the whole list, tiles of 32
+// quartets dealt to the blocks grid-stride; the kernel reads the surviving
+// count from the device, so the same launch serves eager and captured builds.
+int run_fused(hfgpu_handle* h, int c, long long n, double thr, int jonly, cudaStream_t stream) {
+    const ClassKernels& K = CLASS_KERNELS[c];
+    StagedArgs a{};
+    a.quartets = h->d_q + h->coff[c];
+    a.n = (int)n;
+    a.q0 = 0;
+    a.ncls = h->d_ncls;
+    a.cls = c;
+    a.prec = 0;
+    a.bra = h->d_apairs[K.bi];
+    a.ket = h->d_apairs[K.ki];
+    a.prims = h->apsoa;
+    a.boys = h->d_boys;
+    a.boysf = h->d_boysf;
+    a.Pb = h->d_Pb;
+    a.boff = h->d_boff;
+    a.nsh = h->nsh;
+    a.G = h->d_G;
+    a.nb = h->nb;
+    a.thr = thr;
+    a.jonly = jonly;
+    a.stats = h->d_stats + c;
+    const long long tiles = (n + 31) / 32;
+    const int blocks = (int)std::max<long long>(1, std::min<long long>(tiles, (long long)h->nsm * 4 * K.fz_minb));
+    ++h->launches;
+    K.fz64<<<blocks, K.fz_threads, K.fz_smem, stream>>>(a);
+    HF_CHECK(cudaGetLastError());
+    return HFGPU_OK;
+}
+
 int run_staged(hfgpu_handle* h, int c, int prec, long long n, const double* P, double thr, int jonly,
                cudaStream_t stream, double* scratch) {
     const ClassKernels& K = CLASS_KERNELS[c];
+    if (prec == 0 && K.fz64 && !h->no_fused) return run_fused(h, c, n, thr, jonly, stream);
     const size_t st = h->stride[c];
     for (long long q0 = 0; q0 < n; q0 += (long long)st) {
         const int m = (int)std::min<long long>((long long)st, n - q0);
@@ -930,6 +967,7 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
     hfgpu_handle* h = new hfgpu_handle();
     h->nsh = B->nsh;
     h->nb = B->nb;
+    if (const char* e = getenv("HFGPU_FUSED")) h->no_fused = (atoi(e) == 0);
     h->shtyp.assign(B->shtyp, B->shtyp + B->nsh);
     h->nzet.assign(B->nzet, B->nzet + B->nsh);
     h->aosh.assign(B->aosh, B->aosh + B->nsh);
