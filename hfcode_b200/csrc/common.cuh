@@ -591,9 +591,6 @@ struct ClassKernels {
     int scat_smem;                // dynamic shared memory of scat (bytes)
     StagedKernel scat32;          // scatter of FP32 chunks (float rows), or nullptr
     int scat32_smem;
-    // fused FP64 kernel (ERI + J/K in one launch, no scratch), or nullptr
-    StagedKernel fz64;
-    int fz_threads, fz_smem, fz_minb;
     int bi, ki, L, nout;
 };
 

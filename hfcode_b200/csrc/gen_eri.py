@@ -629,251 +629,6 @@ def acc_groups(g: "ClassGen", group: int = ACC_GROUP):
     return best[1]
 
 
-# J/K blocks of the scatter: (name, row centre, col centre, P block, scale)
-# for e(i,j,k,l): J_ab(i,j) += P_cd(k,l) e, J_cd(k,l) += P_ab(i,j) e,
-# K_ac(i,k) += P_bd(j,l) e, K_ad(i,l) += P_bc(j,k) e, K_bc(j,k) += P_ad(i,l) e,
-# K_bd(j,l) += P_ac(i,k) e; J scaled by 2s, K by -s/2 (s: degeneracy weight).
-JK_BLOCKS = [("jab", 0, 1, (2, 3), "sJ"), ("jcd", 2, 3, (0, 1), "sJ"), ("kac", 0, 2, (1, 3), "sK"),
-             ("kad", 0, 3, (1, 2), "sK"), ("kbc", 1, 2, (0, 3), "sK"), ("kbd", 1, 3, (0, 2), "sK")]
-CENTRE = "abcd"
-
-
-def fused_plan(g: "ClassGen", prm: dict):
-    """Work split of the fused kernel of one class: warp w of a block owns a
-    contiguous range of the flat outputs, the J/K elements those outputs
-    touch, and a set of accumulator groups balanced by VRR cost."""
-    nw = prm.get("fz_warps", g.nf[0])
-    per = -(-g.nout // nw)
-    outs_w = [list(range(w * per, min(g.nout, (w + 1) * per))) for w in range(nw)]
-    assert all(outs_w), "every warp needs outputs"
-    elems_w = []
-    for outs in outs_w:
-        seen, lst = set(), []
-        for n in outs:
-            o = g.outputs[n]
-            for bn, r, c, _, _ in JK_BLOCKS:
-                e = (bn, o[r], o[c])
-                if e not in seen:
-                    seen.add(e)
-                    lst.append(e)
-        elems_w.append(lst)
-    groups = acc_groups(g, prm.get("fz_acc_group", ACC_GROUP))
-    cost = [g._vrr_block(set(gr))[2]["vrr"] + len(gr) for gr in groups]
-    load = [0] * nw
-    gw = [[] for _ in range(nw)]
-    for k in sorted(range(len(groups)), key=lambda k: -cost[k]):
-        w = min(range(nw), key=lambda x: load[x])
-        gw[w].append(k)
-        load[w] += cost[k]
-    return nw, outs_w, elems_w, groups, gw
-
-
-def fused_source(g: "ClassGen", prm: dict):
-    """The fused kernel of a staged class (FP64): one launch per class, no
-    scratch in HBM.  A block of NW warps works on tiles of 32 quartets (one
-    per lane), with two shared-memory regions: the accumulators [key][32] and
-    the partial J/K sums [slot][32].
-
-      A  each warp evaluates its accumulator groups (Boys, VRR, contraction)
-         for the 32 quartets and stores them in the accumulator region;
-      B  each warp forms its outputs by HRR and the spherical transform from
-         the shared accumulators, contracts each output at once into the
-         partial J/K sums of the elements it touches, and stores a partial sum
-         in its slot as soon as its last contribution is in (so few stay in
-         registers), with its max|e|;
-      C  the post-screen max|e| < thr is taken over all warps
-         (fock_build_non_diag.f90:69), and each J/K element of each quartet
-         is summed over the warps that touched it and added to G with one
-         FP64 atomic (J_ab summed across the warp first when all 32 quartets
-         share their bra pair).
-
-    Two barriers per tile: after A (accumulators complete) and after B
-    (partial sums complete, accumulators no longer read); C of one tile and A
-    of the next touch disjoint regions.
-    Returns (device functions, kernel, registration lines, info)."""
-    nw, outs_w, elems_w, groups, gw = fused_plan(g, prm)
-    minb = prm.get("fz_minb", 1)
-    tag = g.tag
-    keyidx = {}
-    for gr in groups:
-        for key in gr:
-            keyidx[key] = len(keyidx)
-    nacc = len(keyidx)
-    redoff, nred = [], 0
-    for el in elems_w:
-        redoff.append(nred)
-        nred += len(el)
-    funcs = []
-    # phase A: accumulator groups (the staged3 stage-A code, stride 32 in smem)
-    for r, gr in enumerate(groups):
-        code, _ = g.emit_acc_role(f"fza_{tag}_r{r}", gr)
-        funcs.append(code)
-    # phase B: per warp, outputs -> partial J/K sums, flushed at last use
-    nf = g.nf
-    maxlive = 0
-    for w in range(nw):
-        outs = outs_w[w]
-        last = {}
-        for r, n in enumerate(outs):
-            o = g.outputs[n]
-            for bn, rr, cc, _, _ in JK_BLOCKS:
-                last[(bn, o[rr], o[cc])] = r
-        slot = {e: redoff[w] + j for j, e in enumerate(elems_w[w])}
-        loaded = {}
-
-        def leaf(key):
-            nm = f"L{keyidx[key]}"
-            if key not in loaded:
-                loaded[key] = nm
-                return nm, f"    const double {nm} = src[{keyidx[key]} * 32];"
-            return nm, None
-
-        pvals = set()
-        live = set()
-        peak = [0]
-
-        def store(r, v):
-            o = g.outputs[outs[r]]
-            pre, body, post = [], [], []
-            for bn, rr, cc, (px, py), _ in JK_BLOCKS:
-                pn = f"P{CENTRE[px]}{CENTRE[py]}_{o[px]}_{o[py]}"
-                if pn not in pvals:
-                    pvals.add(pn)
-                    pre.append(f"    const double {pn} = __ldg(B{CENTRE[px]}{CENTRE[py]} + {o[px] * nf[py] + o[py]});")
-                e = (bn, o[rr], o[cc])
-                en = f"{bn}_{o[rr]}_{o[cc]}"
-                if e not in live:
-                    live.add(e)
-                    pre.append(f"    double {en} = 0.0;")
-                body.append(f"      {en} += {pn} * v;")
-                if last[e] == r:
-                    post.append(f"    red[{slot[e]} * 32] = {en};")
-                    live.discard(e)
-            peak[0] = max(peak[0], len(live) + len(post))
-            return "\n".join(pre + [f"    {{ const double v = {v};", "      mx = fmax(mx, fabs(v));"] + body +
-                             ["    }"] + post)
-
-        hlines, _, _ = g._hrr_block(outs, leaf, "double", store)
-        assert not live
-        maxlive = max(maxlive, peak[0])
-        funcs.append("\n".join([
-            f"// ({g.A}{g.B}|{g.C}{g.D}) fused phase B of warp {w}: outputs {outs[0]}..{outs[-1]}, "
-            f"{len(elems_w[w])} J/K elements (at most {peak[0]} partial sums live)",
-            f"__device__ __forceinline__ double fzb_{tag}_w{w}(const GPair& bra, const GPair& ket,",
-            "    const double* __restrict__ src, const double* __restrict__ Bab, const double* __restrict__ Bac,",
-            "    const double* __restrict__ Bad, const double* __restrict__ Bbc, const double* __restrict__ Bbd,",
-            "    const double* __restrict__ Bcd, double* __restrict__ red)",
-            "{",
-            "    double mx = 0.0;"] + hlines + ["    return mx;", "}"]))
-    # phase C: element sums over warps and the atomics, elements dealt to
-    # warps round-robin in the order of the J/K blocks
-    org = {0: "a0", 1: "b0", 2: "c0", 3: "d0"}
-    allel = sorted({e for el in elems_w for e in el},
-                   key=lambda e: ([b[0] for b in JK_BLOCKS].index(e[0]), e[1], e[2]))
-    cw = [[] for _ in range(nw)]
-    for n, e in enumerate(allel):
-        cw[n % nw].append(e)
-    blk = {b[0]: b for b in JK_BLOCKS}
-    for w in range(nw):
-        lines = [f"__device__ __forceinline__ void fzc_{tag}_w{w}(const double* __restrict__ s, const GPair& bra,",
-                 "    const GPair& ket, double* __restrict__ G, int nb, double sJ, double sK, bool act, bool wuni,",
-                 "    int lane, bool jonly)",
-                 "{",
-                 "    const int a0 = bra.aoa, b0 = bra.aob, c0 = ket.aoa, d0 = ket.aob;"]
-        kdone = False
-        for e in cw[w]:
-            bn, i, j = e
-            _, rr, cc, _, sc = blk[bn]
-            if bn[0] == "k" and not kdone:
-                lines.append("    if (jonly) return;")
-                kdone = True
-            slots = [redoff[v] + elems_w[v].index(e) for v in range(nw) if e in elems_w[v]]
-            assert slots and all(0 <= x < nred for x in slots)
-            sm = " + ".join(f"s[{x} * 32]" for x in slots)
-            addr = f"G + ({org[rr]} + {i}) + (size_t)({org[cc]} + {j}) * nb"
-            if bn == "jab":
-                lines.append(f"    {{ double v = act ? {sc} * ({sm}) : 0.0;")
-                lines.append("      if (wuni) {")
-                lines.append("#pragma unroll")
-                lines.append("        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);")
-                lines.append(f"        if (lane == 0) atomicAdd({addr}, v);")
-                lines.append(f"      }} else if (act) atomicAdd({addr}, v); }}")
-            else:
-                lines.append(f"    if (act) atomicAdd({addr}, {sc} * ({sm}));")
-        lines.append("}")
-        funcs.append("\n".join(lines))
-    # the kernel
-    a_calls, b_calls, c_calls = [], [], []
-    base = [0]
-    for gr in groups:
-        base.append(base[-1] + len(gr))
-    for w in range(nw):
-        cond = "if" if w == 0 else "else if"
-        a_calls.append(f"        {cond} (w == {w}) {{")
-        for r in gw[w]:
-            a_calls.append(f"            fza_{tag}_r{r}(bra, ket, a.prims, sboys, sacc + {base[r]} * 32 + lane, 32);")
-        a_calls.append("        }")
-        b_calls.append(f"        {cond} (w == {w}) mx = fzb_{tag}_w{w}(bra, ket, sacc + lane, Bab, Bac, Bad, Bbc, Bbd, "
-                       f"Bcd, sred + lane);")
-        c_calls.append(f"        {cond} (w == {w}) fzc_{tag}_w{w}(sred + lane, bra, ket, a.G, a.nb, sJ, sK, act, wuni, "
-                       f"lane, a.jonly != 0);")
-    kern = f"""
-// Fused (FP64) kernel of class ({g.A}{g.B}|{g.C}{g.D}): {nw} warps, {len(groups)} accumulator groups,
-// {nacc} accumulators and {nred} partial J/K sums per quartet in shared memory.
-__global__ void __launch_bounds__({nw * 32}, {minb}) k_fz_{tag}(StagedArgs a) {{
-    extern __shared__ __align__(16) double hf_fz_smem[];
-    double* const sacc = hf_fz_smem;                        // [{nacc}][32] accumulators
-    double* const sred = hf_fz_smem + {nacc} * 32;           // [{nred}][32] partial J/K sums
-    double* const smx = hf_fz_smem + {nacc + nred} * 32;     // [{nw}][32] max|e| per warp
-    const double* __restrict__ sboys = a.boys + (size_t){g.L} * BOYS_BLK;  // through L1
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int cnt = staged_count(a);
-    const int ntile = (cnt + 31) >> 5;
-    unsigned long long nsc = 0, npr = 0;
-    for (int tile = blockIdx.x; tile < ntile; tile += gridDim.x) {{
-        const int t = (tile << 5) + lane;
-        const bool valid = t < cnt;
-        const uint2 q = staged_quartet(a, valid ? t : (tile << 5));
-        const GPair bra = a.bra[q.x];
-        const GPair ket = a.ket[q.y];
-{chr(10).join(a_calls)}
-        __syncthreads();  // accumulators complete; the previous tile's partial sums are consumed
-        const double* __restrict__ Bab = a.Pb + __ldg(a.boff + bra.sa * a.nsh + bra.sb);
-        const double* __restrict__ Bac = a.Pb + __ldg(a.boff + bra.sa * a.nsh + ket.sa);
-        const double* __restrict__ Bad = a.Pb + __ldg(a.boff + bra.sa * a.nsh + ket.sb);
-        const double* __restrict__ Bbc = a.Pb + __ldg(a.boff + bra.sb * a.nsh + ket.sa);
-        const double* __restrict__ Bbd = a.Pb + __ldg(a.boff + bra.sb * a.nsh + ket.sb);
-        const double* __restrict__ Bcd = a.Pb + __ldg(a.boff + ket.sa * a.nsh + ket.sb);
-        double mx = 0.0;
-{chr(10).join(b_calls)}
-        smx[w * 32 + lane] = mx;
-        __syncthreads();  // partial sums complete; accumulators no longer read
-        double m = 0.0;
-#pragma unroll
-        for (int v = 0; v < {nw}; ++v) m = fmax(m, smx[v * 32 + lane]);
-        const bool act = valid && !(m < a.thr);  // fock_build_non_diag.f90:69
-        const double s = (bra.sa == bra.sb ? 0.5 : 1.0) * (ket.sa == ket.sb ? 0.5 : 1.0);
-        const double sJ = 2.0 * s, sK = -0.5 * s;
-        const unsigned long long bkey = ((unsigned long long)bra.aoa << 32) | (unsigned)bra.aob;
-        const bool wuni = __all_sync(0xffffffffu, bkey == __shfl_sync(0xffffffffu, bkey, 0));
-{chr(10).join(c_calls)}
-        if (w == 0) {{
-            nsc += act ? 1ull : 0ull;
-            npr += valid ? (unsigned long long)(bra.np * ket.np) : 0ull;
-        }}
-    }}
-    if (a.stats && w == 0) warp_add_stats(a.stats, nsc, npr, 0ull);
-}}"""
-    smem = (nacc + nred + nw) * 32 * 8
-    assert smem <= 227 * 1024, (tag, smem)
-    reg = [f"    k->fz64 = k_fz_{tag};", f"    k->fz_threads = {nw * 32};", f"    k->fz_smem = {smem};",
-           f"    k->fz_minb = {minb};"]
-    info = {"fused": {"warps": nw, "groups": len(groups), "nacc": nacc, "nred": nred, "smem": smem, "minb": minb,
-                      "group_sizes": [len(gr) for gr in groups], "max_live_partials": maxlive,
-                      "group_vrr": [g._vrr_block(set(gr))[2]["vrr"] for gr in groups]}}
-    return funcs, kern, reg, info
-
-
 def class_source(ci: int, bi: int, ki: int):
     """Header (device functions) and translation unit (kernels) of one
     quartet class; returns (cuh_text, cu_text, info).
@@ -1036,12 +791,6 @@ __global__ void __launch_bounds__(ND_THREADS) {kname}(StagedArgs a) {{
         assert len(groups) <= MAXR and len(outroles) <= MAXR
     if mode == "staged2":
         assert len(roles) <= MAXR
-    if mode != "direct" and prm.get("fused", False):
-        ff, fk, fr, finfo = fused_source(g, prm)
-        funcs += ff
-        kern.append(fk)
-        reg += fr
-        info.update(finfo)
     info["mode"] = mode
     info["dims"] = [NA, NB, NC, ND]
     if bi != ki:
@@ -1200,36 +949,6 @@ def main(outdir: str):
                 lines.append(f"      for (int i = 0; i < {n}; ++i) out[{outs[0]} + i] = of[i]; }}")
                 lines.append(f"    else hrr_{tag}_r{r}(b, k, acc, out + {outs[0]}, 1);")
         lines.append("}")
-        # the fused kernel's device functions for one quartet (lane 0 of a
-        # tile), the host standing in for the block: phase A for every group,
-        # phase B for every warp, phase C with per-lane atomics
-        fz = info.get("fused")
-        lines.append(f"inline int host_fused_{ci}(const GPair& b, const GPair& k, const PrimSoA& p, const double* t,")
-        lines.append(f"                          const double* Pb, const int* boff, int nsh, double* G, int nb) {{")
-        if fz:
-            tg = info["tag"]
-            lines.append(f"    std::vector<double> sacc({fz['nacc']} * 32), sred({fz['nred']} * 32);")
-            base = 0
-            for r, n in enumerate(fz["group_sizes"]):
-                lines.append(f"    fza_{tg}_r{r}(b, k, p, t, sacc.data() + {base} * 32, 32);")
-                base += n
-            lines.append("    const double* Bab = Pb + boff[b.sa * nsh + b.sb];")
-            lines.append("    const double* Bac = Pb + boff[b.sa * nsh + k.sa];")
-            lines.append("    const double* Bad = Pb + boff[b.sa * nsh + k.sb];")
-            lines.append("    const double* Bbc = Pb + boff[b.sb * nsh + k.sa];")
-            lines.append("    const double* Bbd = Pb + boff[b.sb * nsh + k.sb];")
-            lines.append("    const double* Bcd = Pb + boff[k.sa * nsh + k.sb];")
-            lines.append("    double mx = 0.0;")
-            for w in range(fz["warps"]):
-                lines.append(f"    mx = std::fmax(mx, fzb_{tg}_w{w}(b, k, sacc.data(), Bab, Bac, Bad, Bbc, Bbd, Bcd, "
-                             f"sred.data()));")
-            lines.append("    const double s = (b.sa == b.sb ? 0.5 : 1.0) * (k.sa == k.sb ? 0.5 : 1.0);")
-            for w in range(fz["warps"]):
-                lines.append(f"    fzc_{tg}_w{w}(sred.data(), b, k, G, nb, 2.0 * s, -0.5 * s, mx >= 0.0, false, 0, false);")
-            lines.append("    return 1;")
-        else:
-            lines.append("    return 0;")
-        lines.append("}")
         # the J/K scatter of a full block with stride 1
         na, nb_, nc, nd = info["dims"]
         lines.append(f"inline int host_scatter_{ci}(const double* e, double s, const GPair& b, const GPair& k,")
@@ -1241,9 +960,6 @@ def main(outdir: str):
     lines.append("typedef int (*HostScat)(const double*, double, const GPair&, const GPair&, const double*, double*, int, bool);")
     lines.append("static const HostEri HOST_ERI[] = {" + ", ".join(f"host_eri_{ci}" for ci in flops) + "};")
     lines.append("static const HostScat HOST_SCAT[] = {" + ", ".join(f"host_scatter_{ci}" for ci in flops) + "};")
-    lines.append("typedef int (*HostFused)(const GPair&, const GPair&, const PrimSoA&, const double*, const double*, "
-                 "const int*, int, double*, int);")
-    lines.append("static const HostFused HOST_FUSED[] = {" + ", ".join(f"host_fused_{ci}" for ci in flops) + "};")
     txt = "\n".join(lines) + "\n"
     inc = '#include "../scatter.cuh"\n'
     inc += "".join(f'#include "cls_{ci:02d}_{info["tag"]}.cuh"\n' for ci, info in flops.items())

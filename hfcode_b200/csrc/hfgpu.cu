@@ -294,7 +294,7 @@ struct hfgpu_handle {
     std::vector<int> last_ref;            // lastXX per reference class
     bool have_schwarz = false;
     int timing = 0;
-    int no_fused = 0;                     // 1: fused classes take the staged path (A/B comparisons)
+    int device = 0;                       // the CUDA device current at hfgpu_init
     cudaStream_t stream = nullptr;
     cudaStream_t aux[NSTREAM] = {};    // independent classes run concurrently on these
     cudaEvent_t fork = nullptr, join[NSTREAM] = {};
@@ -329,9 +329,10 @@ struct hfgpu_handle {
     double* d_dscratch = nullptr;  // scratch of the staged diagonal builders
     size_t dstride[NPT] = {};
     size_t scratch_doubles = 0;
+    size_t dscratch_doubles = 0;   // scratch of the staged diagonal builders
     size_t stride[NCLS] = {};      // quartets per chunk of each staged class
     size_t slot_doubles = 0;       // scratch per class stream
-    size_t scratch_budget = 0;     // bytes; 0 = default (HFGPU_SCRATCH_MB or 6 GiB)
+    size_t scratch_budget = 0;     // bytes; 0 = default (HFGPU_SCRATCH_MB, or 24 GiB capped at device memory / 6)
     size_t naprims = 0;            // primitive pairs of the active lists
     unsigned long long* d_cnt = nullptr;
     ClassStats* d_stats = nullptr;
@@ -403,8 +404,6 @@ struct ClassTable {
                 cudaFuncSetAttribute(k[c].scat, cudaFuncAttributeMaxDynamicSharedMemorySize, k[c].scat_smem);
             if (k[c].scat32 && k[c].scat32_smem > 0)
                 cudaFuncSetAttribute(k[c].scat32, cudaFuncAttributeMaxDynamicSharedMemorySize, k[c].scat32_smem);
-            if (k[c].fz64 && k[c].fz_smem > 0)
-                cudaFuncSetAttribute(k[c].fz64, cudaFuncAttributeMaxDynamicSharedMemorySize, k[c].fz_smem);
         }
     }
 };
@@ -521,8 +520,6 @@ int launch_diag(hfgpu_handle* h, int mode, const double* P, double thr, double* 
     return HFGPU_OK;
 }
 
-// Scratch budget of the staged classes in doubles (default 6 GiB; the
-// HFGPU_SCRATCH_MB environment variable overrides it).
 // Default scratch budget: 24 GiB, at most a sixth of the device's memory.
 // Larger chunks mean fewer role/scatter launches per class and shorter
 // tails: C60 builds 226.3 ms at 6 GiB, 220.5 ms at 24 GiB.  A handle
@@ -732,43 +729,9 @@ int build_active(hfgpu_handle* h) {
 
 // Staged class: chunks of the quartet list through the accumulator roles
 // (mode 2), the output roles and the scatter kernel.
-// Fused class (FP64 quartets): one launch over the whole list, tiles of 32
-// quartets dealt to the blocks grid-stride; the kernel reads the surviving
-// count from the device, so the same launch serves eager and captured builds.
-int run_fused(hfgpu_handle* h, int c, long long n, double thr, int jonly, cudaStream_t stream) {
-    const ClassKernels& K = CLASS_KERNELS[c];
-    StagedArgs a{};
-    a.quartets = h->d_q + h->coff[c];
-    a.n = (int)n;
-    a.q0 = 0;
-    a.ncls = h->d_ncls;
-    a.cls = c;
-    a.prec = 0;
-    a.bra = h->d_apairs[K.bi];
-    a.ket = h->d_apairs[K.ki];
-    a.prims = h->apsoa;
-    a.boys = h->d_boys;
-    a.boysf = h->d_boysf;
-    a.Pb = h->d_Pb;
-    a.boff = h->d_boff;
-    a.nsh = h->nsh;
-    a.G = h->d_G;
-    a.nb = h->nb;
-    a.thr = thr;
-    a.jonly = jonly;
-    a.stats = h->d_stats + c;
-    const long long tiles = (n + 31) / 32;
-    const int blocks = (int)std::max<long long>(1, std::min<long long>(tiles, (long long)h->nsm * 4 * K.fz_minb));
-    ++h->launches;
-    K.fz64<<<blocks, K.fz_threads, K.fz_smem, stream>>>(a);
-    HF_CHECK(cudaGetLastError());
-    return HFGPU_OK;
-}
-
 int run_staged(hfgpu_handle* h, int c, int prec, long long n, const double* P, double thr, int jonly,
                cudaStream_t stream, double* scratch) {
     const ClassKernels& K = CLASS_KERNELS[c];
-    if (prec == 0 && K.fz64 && !h->no_fused) return run_fused(h, c, n, thr, jonly, stream);
     const size_t st = h->stride[c];
     for (long long q0 = 0; q0 < n; q0 += (long long)st) {
         const int m = (int)std::min<long long>((long long)st, n - q0);
@@ -967,7 +930,6 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
     hfgpu_handle* h = new hfgpu_handle();
     h->nsh = B->nsh;
     h->nb = B->nb;
-    if (const char* e = getenv("HFGPU_FUSED")) h->no_fused = (atoi(e) == 0);
     h->shtyp.assign(B->shtyp, B->shtyp + B->nsh);
     h->nzet.assign(B->nzet, B->nzet + B->nsh);
     h->aosh.assign(B->aosh, B->aosh + B->nsh);
@@ -999,6 +961,7 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
     {
         int dev = 0;
         if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, dev);
+        h->device = dev;
         if (h->nsm <= 0) h->nsm = 148;
     }
     int rc = 0;
@@ -1080,10 +1043,9 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
         hfgpu_finalize(h);
         return set_err(HFGPU_ERR_CUDA, m);
     }
-    // staged diagonal builders: (i, i) lists and their scratch
+    // staged diagonal builders: (i, i) lists (their scratch is sized by the
+    // handle's budget at the first fock_build_initial_diag)
     {
-        size_t need = 0;
-        const size_t budget = scratch_budget_doubles();
         for (int t = 0; t < NPT && ce == cudaSuccess; ++t) {
             const ClassKernels& K = CLASS_KERNELS[class_index(t, t)];
             const size_t n = h->pairs[t].size();
@@ -1095,14 +1057,6 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
                 return HFGPU_ERR_NOMEM;
             }
             ce = up(h->d_diaglist[t], dl.data(), n * sizeof(uint2));
-            const size_t per = (size_t)K.nacc + K.nout + K.nrole_b;
-            size_t st = std::max<size_t>(std::min<size_t>(n, budget / per), 128);
-            h->dstride[t] = st;
-            need = std::max(need, st * per);
-        }
-        if (ce == cudaSuccess && need && dalloc(&h->d_dscratch, need)) {
-            hfgpu_finalize(h);
-            return HFGPU_ERR_NOMEM;
         }
     }
     if (ce == cudaSuccess) ce = cudaMemset(h->d_stats, 0, NCLS * sizeof(ClassStats));
@@ -1148,6 +1102,28 @@ int hfgpu_finalize(hfgpu_handle* h) {
     return HFGPU_OK;
 }
 
+// Scratch of the staged diagonal builders (one chunk of stride pairs holds
+// accumulators, outputs and role maxima per pair), sized once per handle by
+// its scratch budget (hfgpu_set_scratch_budget, else the default).
+static int alloc_diag_scratch(hfgpu_handle* h) {
+    if (h->d_dscratch) return HFGPU_OK;
+    const size_t budget = h->scratch_budget ? h->scratch_budget / sizeof(double) : scratch_budget_doubles();
+    size_t need = 0;
+    for (int t = 0; t < NPT; ++t) {
+        const ClassKernels& K = CLASS_KERNELS[class_index(t, t)];
+        const size_t n = h->pairs[t].size();
+        if (K.mode == 0 || n == 0) continue;
+        const size_t per = (size_t)K.nacc + K.nout + K.nrole_b;
+        const size_t st = std::max<size_t>(std::min<size_t>(n, budget / per), 128);
+        h->dstride[t] = st;
+        need = std::max(need, st * per);
+    }
+    if (!need) return HFGPU_OK;
+    const int rc = dalloc(&h->d_dscratch, need);
+    if (rc == HFGPU_OK) h->dscratch_doubles = need;
+    return rc;
+}
+
 static void drop_graph(hfgpu_handle* h) {
     if (h->gexec) cudaGraphExecDestroy(h->gexec);
     if (h->graph) cudaGraphDestroy(h->graph);
@@ -1160,6 +1136,8 @@ int hfgpu_fock_build_initial_diag(hfgpu_handle* h, double* f, const double* p, d
     {
         HF_DEVICE_LOCK;
         drop_graph(h);  // the Schwarz pass re-sizes the buffers a captured build points at
+        const int rc = alloc_diag_scratch(h);
+        if (rc) return rc;
     }
     int rc = upload_fp(h, f, p);
     if (rc) return rc;
@@ -1410,6 +1388,7 @@ int hfgpu_device_bytes(const hfgpu_handle* h, size_t* bytes) {
     b += 8 * h->naprims * sizeof(double);                     // active-list primitives
     b += h->qcap * sizeof(uint2);                             // quartet lists
     b += h->scratch_doubles * sizeof(double);                 // staged scratch
+    b += h->dscratch_doubles * sizeof(double);                // staged diagonal builders' scratch
     b += h->subcap * (sizeof(ScreenSub) + 2 * sizeof(unsigned long long));
     b += (size_t)(BOYS_MMAX + 1) * BOYS_BLK * (sizeof(double) + sizeof(float));
     *bytes = b;
@@ -1520,7 +1499,7 @@ int hfgpu_measure_fma_peak(double* fp64_gflops, double* fp32_gflops) {
 // Scratch of hfgpu_fock_build_diag_static: the one-triangle accumulation
 // buffer G (nb x nb) and the shell-pair density maxima (nsh x nsh) live in
 // this file-scope device array instead of memory from cudaMalloc.  Every GPU
-// that loads the library holds it (10.1 MB) until the process exits.
+// that loads the library holds it (10,485,760 bytes, 10.0 MiB) until the process exits.
 namespace {
 constexpr int STATIC_MAX_NB = 1024;
 constexpr int STATIC_MAX_NSH = 512;
@@ -1564,6 +1543,14 @@ extern "C" int hfgpu_fock_build_diag_static(hfgpu_handle* h, double* f_dev, cons
                                           std::to_string(STATIC_MAX_NB) + ", nsh <= " +
                                           std::to_string(STATIC_MAX_NSH));
     if (!h->have_schwarz) return set_err(HFGPU_ERR_STATE, "fock_build_initial_diag has not been called");
+    {
+        int dev = -1;
+        HF_CHECK(cudaGetDevice(&dev));
+        if (dev != h->device)
+            return set_err(HFGPU_ERR_ARG, "hfgpu_fock_build_diag_static: the current device (" + std::to_string(dev) +
+                                              ") is not the device the handle was created on (" +
+                                              std::to_string(h->device) + ")");
+    }
     double* scratch = nullptr;
     int rc = static_scratch(&scratch);
     if (rc) return rc;

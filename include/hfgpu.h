@@ -4,7 +4,7 @@
  * Drop-in boundary for the reference's Fock builders.  Each entry point
  * replaces one external subroutine of brichjnh/hfcode that
  * direct_hartreefock.f90 calls (direct_hartreefock.f90:101-121); the
- * Fortran side binds them through iso_c_binding.
+ * Fortran side binds them through an iso_c_binding interface module.
  *
  * Conventions shared by all entry points
  *   - f and p are caller-owned HOST arrays of nb x nb doubles, column-major
@@ -195,7 +195,7 @@ int hfgpu_one_electron_gpu(const hfgpu_basis* basis, int natom, const double* ch
  * not allowed, or that must not grow the device footprint after start-up.
  * No counterpart in the reference.  It allocates nothing: its scratch (the
  * accumulation buffer and the shell-pair density maxima) is a file-scope
- * __device__ array of 10.1 MB that every GPU loading the library holds until
+ * __device__ array of 10,485,760 bytes (10.0 MiB) that every GPU loading the library holds until
  * exit, so nb <= 1024 and nsh <= 512 (larger sizes return HFGPU_ERR_ARG).
  * f_dev += G_diag(p_dev), enqueued on the handle's stream.  The handle must
  * come from hfgpu_init + hfgpu_fock_build_initial_diag, called earlier where

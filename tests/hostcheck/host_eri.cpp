@@ -7,7 +7,6 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <algorithm>
 #include <vector>
 
 #define __device__
@@ -20,7 +19,6 @@ static inline double rsqrt(double x) { return 1.0 / std::sqrt(x); }
 static inline float rsqrtf(float x) { return 1.0f / std::sqrt(x); }
 template <class T>
 static inline T __ldg(const T* p) { return *p; }
-static inline double __shfl_xor_sync(unsigned, double v, int) { return v; }
 static inline double atomicAdd(double* p, double v) {
     double o = *p;
     *p += v;
@@ -94,41 +92,6 @@ int hc_scatter(void* hh, int cls, int a, int b, int c, int d, const double* e, d
     GPair bra = make_pair(h->B, a, b, prims);
     GPair ket = make_pair(h->B, c, d, prims);
     return HOST_SCAT[cls](e, s, bra, ket, P, G, nb, jonly != 0);
-}
-
-
-// The fused kernel's arithmetic for one quartet (returns 0 when the class has
-// no fused kernel): P column-major nb x nb, laid out in shell-pair blocks as
-// the library does, G accumulated column-major.
-int hc_fused(void* hh, int cls, int L, int a, int b, int c, int d, const double* P, double* G, int nb) {
-    HC* h = (HC*)hh;
-    const hfgpu_basis* B = h->B;
-    const int nsh = B->nsh;
-    std::vector<int> nf(nsh), boff((size_t)nsh * nsh);
-    for (int s = 0; s < nsh; ++s) {
-        const int t = B->shtyp[s];
-        nf[s] = t == HFGPU_SHELL_S ? 1 : t == HFGPU_SHELL_P ? 3 : t == HFGPU_SHELL_D ? 5 : 4;
-    }
-    int off = 0;
-    for (int s1 = 0; s1 < nsh; ++s1)
-        for (int s2 = 0; s2 < nsh; ++s2) {
-            boff[(size_t)s1 * nsh + s2] = off;
-            off += nf[s1] * nf[s2];
-        }
-    std::vector<double> Pb(off);
-    for (int s1 = 0; s1 < nsh; ++s1)
-        for (int s2 = 0; s2 < nsh; ++s2)
-            for (int i = 0; i < nf[s1]; ++i)
-                for (int j = 0; j < nf[s2]; ++j)
-                    Pb[boff[(size_t)s1 * nsh + s2] + i * nf[s2] + j] =
-                        P[(B->aosh[s1] + i) + (size_t)(B->aosh[s2] + j) * nb];
-    std::vector<GPrim> prims;
-    GPair bra = make_pair(B, a, b, prims);
-    GPair ket = make_pair(B, c, d, prims);
-    std::vector<double> soa = prims_soa(prims);
-    const PrimSoA ps = soa_view(soa.data(), prims.size());
-    const double* t = h->bt.data() + (size_t)L * BOYS_BLK;
-    return HOST_FUSED[cls](bra, ket, ps, t, Pb.data(), boff.data(), nsh, G, nb);
 }
 
 }

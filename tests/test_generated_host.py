@@ -61,8 +61,6 @@ def _build():
     lib.hc_scatter.argtypes = [vp, i, i, i, i, i, d, ctypes.c_double, d, d, i, i]
     lib.hc_scatter.restype = i
     lib.hc_boys.argtypes = [vp, i, ctypes.c_double, d]
-    lib.hc_fused.argtypes = [vp, i, i, i, i, i, i, d, d, i]
-    lib.hc_fused.restype = i
     return lib, json.load(open(os.path.join(GEN, "class_flops.json")))
 
 
@@ -167,42 +165,3 @@ def test_device_boys_matches_exact(host):
             ref = mdref.boys_ref_longrange(M, float(T))
             rel = np.max(np.abs(out[:M + 1] - ref) / np.abs(ref))
             assert rel < 5e-14, (M, T, rel)
-
-
-def test_fused_kernel_arithmetic_matches_uniform_scatter(host):
-    """The fused classes' device functions (accumulator groups, per-warp HRR
-    with partial J/K sums flushed to shared slots, per-element sums over the
-    warps), run for one quartet on the host, against the oracle's ERI block
-    contracted with the uniform degeneracy-weighted scatter."""
-    lib, info = host
-    _, _, sh, _ = system("alkane2_mix")
-    desc = BasisDescriptor(sh)
-    h = lib.hc_create(ctypes.addressof(desc.struct))
-    orc = pyoracle.Oracle(sh)
-    nb = sh.nb
-    rng = np.random.default_rng(13)
-    P = rng.normal(size=(nb, nb))
-    P = np.asfortranarray(P + P.T)
-    checked = 0
-    for ci, qs in class_quartets(sh, rng, n=2).items():
-        if not info[str(ci)].get("fused"):
-            continue
-        for q in qs:
-            e = orc.eri(*q)
-            na, nb_, nc, nd = (NFUNC[int(sh.shtyp[x])] for x in q)
-            E = e.reshape(na, nb_, nc, nd)
-            s = (0.5 if q[0] == q[1] else 1.0) * (0.5 if q[2] == q[3] else 1.0)
-            G = np.zeros((nb, nb), order="F")
-            assert lib.hc_fused(h, ci, info[str(ci)]["L"], *q, _dp(P), _dp(G), nb) == 1
-            o = [int(sh.aosh[x]) for x in q]
-            R = np.zeros((nb, nb), order="F")
-            sl = [slice(o[k], o[k] + n) for k, n in enumerate((na, nb_, nc, nd))]
-            R[sl[0], sl[1]] += 2 * s * np.einsum("ijkl,kl->ij", E, P[sl[2], sl[3]])
-            R[sl[2], sl[3]] += 2 * s * np.einsum("ijkl,ij->kl", E, P[sl[0], sl[1]])
-            R[sl[0], sl[2]] -= 0.5 * s * np.einsum("ijkl,jl->ik", E, P[sl[1], sl[3]])
-            R[sl[0], sl[3]] -= 0.5 * s * np.einsum("ijkl,jk->il", E, P[sl[1], sl[2]])
-            R[sl[1], sl[2]] -= 0.5 * s * np.einsum("ijkl,il->jk", E, P[sl[0], sl[3]])
-            R[sl[1], sl[3]] -= 0.5 * s * np.einsum("ijkl,ik->jl", E, P[sl[0], sl[2]])
-            assert np.max(np.abs(G - R)) < 1e-12 * max(1.0, np.max(np.abs(R))), (info[str(ci)]["name"], q)
-            checked += 1
-    assert checked > 0
