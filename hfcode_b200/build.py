@@ -18,6 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(CSRC, "_build")
 LIB = os.path.join(HERE, "libhfgpu.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+CUDA_LIB = os.path.join(os.path.dirname(os.path.dirname(NVCC)), "lib64")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-v"]
 
@@ -55,8 +56,9 @@ def build(jobs: int = 0, verbose: bool = True) -> str:
               os.path.join(HERE, "..", "include", "hfgpu.h"),
               os.path.join(HERE, "..", "include", "hfgpu_basis.h"),
               os.path.join(HERE, "..", "include", "hfgpu_ingest.h"),
+              os.path.join(HERE, "..", "include", "hfgpu_scf.h"),
               os.path.join(CSRC, "generated", "class_table.inc")]
-    srcs = [os.path.join(CSRC, "hfgpu.cu"), os.path.join(CSRC, "onee.cu"),
+    srcs = [os.path.join(CSRC, "hfgpu.cu"), os.path.join(CSRC, "onee.cu"), os.path.join(CSRC, "scf.cu"),
             os.path.join(CSRC, "ingest.cpp")] + sorted(gen_srcs)
     objs = [os.path.join(BUILD, os.path.splitext(os.path.basename(s))[0] + ".o") for s in srcs]
     jobs = jobs or max(1, min(len(srcs), os.cpu_count() or 4))
@@ -68,7 +70,9 @@ def build(jobs: int = 0, verbose: bool = True) -> str:
             if done and verbose:
                 print("compiled", os.path.basename(done), flush=True)
     if _newer(LIB, objs):
-        subprocess.check_call([NVCC] + ARCH + ["-shared", "-o", LIB] + objs)
+        # cuBLAS and cuSOLVER serve the device SCF step (scf.cu)
+        subprocess.check_call([NVCC] + ARCH + ["-shared", "-o", LIB] + objs +
+                              ["-lcublas", "-lcusolver", "-Xlinker", "-rpath=" + CUDA_LIB])
     return LIB
 
 

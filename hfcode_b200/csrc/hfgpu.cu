@@ -1204,6 +1204,32 @@ int hfgpu_fock_build_device(hfgpu_handle* h, double* f_dev, const double* p_dev,
     return device_build(h, f_dev, p_dev, thr_diag, thr_non_diag, fp32_cutoff, false);
 }
 
+int hfgpu_fock_build_initial_diag_device(hfgpu_handle* h, double* f_dev, const double* p_dev, double thr) {
+    if (!h || !f_dev || !p_dev) return set_err(HFGPU_ERR_ARG, "null argument");
+    {
+        HF_DEVICE_LOCK;
+        drop_graph(h);  // the Schwarz pass re-sizes the buffers a captured build points at
+        const int rc = alloc_diag_scratch(h);
+        if (rc) return rc;
+    }
+    HF_CHECK(cudaMemsetAsync(h->d_G, 0, (size_t)h->nb * h->nb * sizeof(double), h->stream));
+    int rc = launch_diag(h, 0, p_dev, thr);
+    if (rc) return rc;
+    if ((rc = launch_symm(h, f_dev))) return rc;
+    return build_active(h);  // reads the Schwarz factors back (synchronises the handle's stream)
+}
+
+int hfgpu_fock_build_non_diag_device(hfgpu_handle* h, double* f_dev, const double* p_dev, double thr,
+                                     double fp32_cutoff) {
+    if (!h || !f_dev || !p_dev) return set_err(HFGPU_ERR_ARG, "null argument");
+    if (!h->have_schwarz) return set_err(HFGPU_ERR_STATE, "fock_build_initial_diag has not been called");
+    HF_CHECK(cudaMemsetAsync(h->d_G, 0, (size_t)h->nb * h->nb * sizeof(double), h->stream));
+    int rc;
+    if ((rc = launch_maxdm(h, p_dev))) return rc;
+    if ((rc = run_non_diag(h, p_dev, thr, 0, fp32_cutoff))) return rc;
+    return launch_symm(h, f_dev);
+}
+
 int hfgpu_graph_capture(hfgpu_handle* h, double* f_dev, const double* p_dev, double thr_diag, double thr_non_diag,
                         double fp32_cutoff) {
     if (!h || !f_dev || !p_dev) return set_err(HFGPU_ERR_ARG, "null argument");

@@ -50,6 +50,20 @@ class HfgpuError(RuntimeError):
 DEVICE_LOCK = threading.RLock()
 
 
+class ScfParams(ctypes.Structure):
+    """hfgpu_scf_params (include/hfgpu_scf.h)."""
+    _fields_ = [("maxiter", ctypes.c_int), ("conv", ctypes.c_double), ("conve", ctypes.c_double),
+                ("lowthresh", ctypes.c_double), ("fdifffac", ctypes.c_double), ("fp32_cutoff", ctypes.c_double),
+                ("levshft", ctypes.c_double)]
+
+
+class ScfResult(ctypes.Structure):
+    """hfgpu_scf_result (include/hfgpu_scf.h)."""
+    _fields_ = [("energy", ctypes.c_double), ("eelec", ctypes.c_double), ("deltae", ctypes.c_double),
+                ("deltap", ctypes.c_double), ("cycles", ctypes.c_int), ("converged", ctypes.c_int),
+                ("full_builds", ctypes.c_int), ("delta_builds", ctypes.c_int)]
+
+
 def _load():
     if not os.path.exists(LIBPATH):
         raise ImportError(f"hfcode_b200: CUDA library {LIBPATH} is missing; run __graft_entry__.build()")
@@ -86,6 +100,15 @@ def _load():
     lib.hfgpu_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp)]
     lib.hfgpu_batch_launch.argtypes = [vp, vp]
     lib.hfgpu_batch_destroy.argtypes = [vp]
+    lib.hfgpu_fock_build_initial_diag_device.argtypes = [vp, vp, vp, ctypes.c_double]
+    lib.hfgpu_fock_build_non_diag_device.argtypes = [vp, vp, vp, ctypes.c_double, ctypes.c_double]
+    lib.hfgpu_scf_defaults.argtypes = [ctypes.POINTER(ScfParams)]
+    lib.hfgpu_scf_defaults.restype = None
+    lib.hfgpu_scf_create.argtypes = [vp, ctypes.c_int, ctypes.c_double, d, d, d, ctypes.POINTER(vp)]
+    lib.hfgpu_scf_run.argtypes = [vp, ctypes.POINTER(ScfParams), ctypes.POINTER(ScfResult)]
+    lib.hfgpu_scf_get.argtypes = [vp, d, d, d]
+    lib.hfgpu_scf_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
+    lib.hfgpu_scf_destroy.argtypes = [vp]
     return lib
 
 
@@ -100,7 +123,10 @@ EXPORTS = ["hfgpu_init", "hfgpu_fock_build_initial_diag", "hfgpu_fock_build_diag
            "hfgpu_device_bytes", "hfgpu_graph_capture", "hfgpu_graph_launch", "hfgpu_synchronize",
            "hfgpu_fock_build_graph", "hfgpu_launch_count", "hfgpu_fock_build_device_on",
            "hfgpu_small_solve", "hfgpu_one_electron_gpu",
-           "hfgpu_batch_create", "hfgpu_batch_launch", "hfgpu_batch_destroy"]
+           "hfgpu_batch_create", "hfgpu_batch_launch", "hfgpu_batch_destroy",
+           "hfgpu_fock_build_initial_diag_device", "hfgpu_fock_build_non_diag_device",
+           "hfgpu_scf_defaults", "hfgpu_scf_create", "hfgpu_scf_run", "hfgpu_scf_get", "hfgpu_scf_device_bytes",
+           "hfgpu_scf_destroy"]
 
 
 def measure_fma_peak():
@@ -260,6 +286,60 @@ class FockBuilder:
         out = {k: np.array(list(a), dtype=np.int64) for k, a in zip(keys, arrs)}
         out["ms"] = np.array(list(ms))
         return out
+
+
+class DeviceSCFJob:
+    """One RHF job whose state stays on the GPU (include/hfgpu_scf.h): the
+    reference's SCF protocol run by the library from C++ on the builder's
+    stream, cuSOLVER's syevd in the role of dsyev.  `builder` is a fresh
+    FockBuilder (no initial diag yet); S and hcore = T + V are host arrays;
+    p_guess None means the core-Hamiltonian guess."""
+
+    def __init__(self, builder: "FockBuilder", nocc: int, enuc: float, S: np.ndarray, hcore: np.ndarray,
+                 p_guess: Optional[np.ndarray] = None):
+        self.builder = builder  # keeps the handle alive
+        self.nb = builder.nb
+        Sc = np.ascontiguousarray(S, dtype=np.float64)
+        Hc = np.ascontiguousarray(hcore, dtype=np.float64)
+        Pc = None if p_guess is None else np.ascontiguousarray(p_guess, dtype=np.float64)
+        out = ctypes.c_void_p()
+        with DEVICE_LOCK:
+            _check(_lib.hfgpu_scf_create(builder.h, int(nocc), float(enuc), _dp(Sc), _dp(Hc),
+                                         _dp(Pc) if Pc is not None else None, ctypes.byref(out)), "scf_create")
+        self.s = out
+
+    def run(self, maxiter: int = 25, conv: float = 1e-5, conve: float = 5e-8, fp32_cutoff: float = 0.0,
+            levshft: float = 0.0, lowthresh: float = 5e-7, fdifffac: float = 0.1) -> Dict[str, float]:
+        """Cycles until convergence or `maxiter` cycles in all (a later call
+        continues); returns the state after the last cycle."""
+        prm = ScfParams(int(maxiter), float(conv), float(conve), float(lowthresh), float(fdifffac),
+                        float(fp32_cutoff), float(levshft))
+        res = ScfResult()
+        _check(_lib.hfgpu_scf_run(self.s, ctypes.byref(prm), ctypes.byref(res)), "scf_run")
+        return {k: getattr(res, k) for k, _ in ScfResult._fields_}
+
+    def get(self):
+        """(P, F, orbital energies) as host arrays."""
+        p, f, e = np.zeros((self.nb, self.nb)), np.zeros((self.nb, self.nb)), np.zeros(self.nb)
+        _check(_lib.hfgpu_scf_get(self.s, _dp(p), _dp(f), _dp(e)), "scf_get")
+        return p, f, e
+
+    def device_bytes(self) -> int:
+        b = ctypes.c_size_t()
+        _check(_lib.hfgpu_scf_device_bytes(self.s, ctypes.byref(b)), "scf_device_bytes")
+        return int(b.value)
+
+    def close(self):
+        if getattr(self, "s", None):
+            with DEVICE_LOCK:
+                _lib.hfgpu_scf_destroy(self.s)
+            self.s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Batch:

@@ -204,3 +204,26 @@ def direct_hartreefock(mol: Molecule, sh: ShellSet, builder, p_guess: Optional[n
         p = 2.0 * cmat[:, :nocc] @ cmat[:, :nocc].T
     return SCFResult(energy=eelec + unuc, eelec=eelec, enuc=unuc, converged=converged, cycles=len(hist),
                      P=p, F=faobold, eigs=eigs, history=hist)
+
+
+def device_hartreefock(mol: Molecule, sh: ShellSet, builder, p_guess: Optional[np.ndarray] = None,
+                       maxiter: int = 25, conv: float = 1e-5, conve: float = 5e-8, fp32_cutoff: float = 0.0,
+                       levshft: Optional[float] = None, ints=None) -> SCFResult:
+    """The same protocol with the job's state on the GPU (fock.DeviceSCFJob):
+    S^-1/2, the densities, Fock matrices and DIIS histories stay in device
+    memory and every cycle runs from the library's C++ on the builder's
+    stream; the host only starts the run and reads the result.  S, T, V come
+    from the GPU one-electron integrals unless `ints` is given."""
+    from . import fock
+    S, T, V = ints if ints is not None else onee.one_electron(mol, sh, gpu=True)
+    job = fock.DeviceSCFJob(builder, mol.nocc, mol.nuclear_repulsion(), S, T + V, p_guess)
+    try:
+        r = job.run(maxiter=maxiter, conv=conv, conve=conve, fp32_cutoff=fp32_cutoff,
+                    levshft=levshft if levshft is not None else 0.0)
+        P, F, eigs = job.get()
+    finally:
+        job.close()
+    return SCFResult(energy=r["energy"], eelec=r["eelec"], enuc=r["energy"] - r["eelec"],
+                     converged=bool(r["converged"]), cycles=r["cycles"], P=P, F=F, eigs=eigs,
+                     history=[{"full_builds": r["full_builds"], "delta_builds": r["delta_builds"],
+                               "deltae": r["deltae"], "deltap": r["deltap"]}])

@@ -7,10 +7,12 @@ serves a stream of jobs on one B200:
   free and its estimated footprint (pair data, screening tables, quartet
   lists, scratch, F/P/G) fits the remaining budget; after the job's
   Schwarz pass the estimate is replaced by the handle's actual usage;
-* each admitted job keeps its Fock-build state resident on the device
-  (its own FockBuilder handle and CUDA streams) and runs the reference's SCF
-  protocol (scf.direct_hartreefock) in a worker thread; the ctypes calls
-  release the GIL, so the builds of concurrent jobs overlap on the GPU;
+* each admitted job keeps its whole state resident on the device -- its own
+  FockBuilder handle (screening tables, quartet lists, CUDA streams) and a
+  device SCF job (density, Fock matrices, DIIS histories, S^-1/2; the
+  library's C++ runs every cycle, include/hfgpu_scf.h) -- in a worker
+  thread; the ctypes calls release the GIL, so concurrent jobs overlap on
+  the GPU and no per-cycle work waits on Python;
 * requests that arrive while others run wait in a FIFO and are admitted as
   slots and memory free up (continuous batching, not a batch barrier);
 * metrics: jobs/s over the stream and per-job latency (arrival -> result)
@@ -82,13 +84,14 @@ def estimate_footprint(sh: ShellSet, scratch_budget: int) -> int:
     quartets = npairs * (npairs - 1) // 2 + npairs
     b = 3 * nb * nb * 8 + nsh * nsh * 8 + 2 * 7 * 8 * nprim + npairs * 200 + quartets * 8
     b += min(scratch_budget, quartets * 8 * 700)
+    b += (13 + 2 * 8) * nb * nb * 8 + (8 << 20)  # device SCF state (hfgpu_scf_create) and its workspaces
     return int(b + (64 << 20))  # + CUDA context share / streams / tables
 
 
 class Server:
     def __init__(self, hbm_budget: int, max_slots: int = 8, scratch_budget: int = 256 << 20,
                  fp32_cutoff: float = 1e-7, conve: float = 1e-8, conv: float = 1e-6, basis_name: str = "6-31G(d)",
-                 graphs: bool = False):
+                 graphs: bool = False, step: str = "device"):
         from . import fock  # loads the CUDA library; fails loudly without it
         self.fock = fock
         self.hbm_budget = hbm_budget
@@ -102,6 +105,12 @@ class Server:
         # under the library's device lock) cost more than the launches they
         # save (measured 7.8 vs 11.9 jobs/s, 200 jobs, 8 slots)
         self.graphs = graphs
+        # "device": the SCF cycle runs in the library's C++ with the job's
+        # state on the GPU; "host": scf.direct_hartreefock (numpy/LAPACK
+        # between builds, the state on the host)
+        if step not in ("device", "host"):
+            raise ValueError("step must be 'device' or 'host'")
+        self.step = step
         self.basis = basismod.load_basis(basis_name)
         self.lock = threading.Condition()
         self.in_use = 0
@@ -137,6 +146,8 @@ class Server:
             self.lock.notify_all()
 
     def run_job(self, job: Job, t0: float):
+        if self.step == "device":
+            return self._run_job_device(job, t0)
         fb = None
         try:
             fb = self.fock.FockBuilder(job.sh, scratch_budget=self.scratch_budget)
@@ -163,6 +174,27 @@ class Server:
         except Exception as e:  # the job fails, the server keeps serving
             job.error = f"{type(e).__name__}: {e}"
         finally:
+            if fb is not None:
+                fb.close()
+            job.finished = time.perf_counter() - t0
+            self._release(job.footprint)
+
+    def _run_job_device(self, job: Job, t0: float):
+        fb = dj = None
+        try:
+            fb = self.fock.FockBuilder(job.sh, scratch_budget=self.scratch_budget)
+            S, T, V = onee.one_electron(job.mol, job.sh, gpu=True)
+            dj = self.fock.DeviceSCFJob(fb, job.mol.nocc, job.mol.nuclear_repulsion(), S, T + V, job.p0)
+            kw = dict(conve=self.conve, conv=self.conv, fp32_cutoff=self.fp32_cutoff)
+            dj.run(maxiter=1, **kw)  # cycle 1: the Schwarz pass sizes the handle's lists and scratch
+            self._adjust(job, fb.device_bytes() + dj.device_bytes() + (64 << 20))
+            r = dj.run(maxiter=60, **kw)
+            job.energy, job.cycles, job.converged = r["energy"], r["cycles"], bool(r["converged"])
+        except Exception as e:  # the job fails, the server keeps serving
+            job.error = f"{type(e).__name__}: {e}"
+        finally:
+            if dj is not None:
+                dj.close()
             if fb is not None:
                 fb.close()
             job.finished = time.perf_counter() - t0
@@ -254,17 +286,18 @@ def main():
     ap.add_argument("--hbm-gb", type=float, default=64.0)
     ap.add_argument("--fp32-cutoff", type=float, default=1e-7)
     ap.add_argument("--sequential", action="store_true", help="also run the plain per-job form")
-    ap.add_argument("--graphs", action="store_true", help="builds after the first as CUDA-graph replays")
+    ap.add_argument("--graphs", action="store_true", help="host step: builds after the first as graph replays")
+    ap.add_argument("--step", default="device", choices=["device", "host"])
     args = ap.parse_args()
     srv = Server(int(args.hbm_gb * (1 << 30)), args.slots, fp32_cutoff=args.fp32_cutoff,
-                 graphs=args.graphs)
+                 graphs=args.graphs, step=args.step)
     jobs = make_stream(args.jobs, args.rate)
     out = {"served": srv.serve(jobs)}
     if args.sequential:
         seq = make_stream(args.jobs, args.rate)
         out["sequential"] = serve_sequential(seq, Server(int(args.hbm_gb * (1 << 30)), 1,
                                                         fp32_cutoff=args.fp32_cutoff,
-                                                        graphs=args.graphs))
+                                                        graphs=args.graphs, step=args.step))
     print(json.dumps(out))
 
 

@@ -79,6 +79,15 @@ int hfgpu_fock_build_non_diag_mixed(hfgpu_handle* h, double* f, const double* p,
 int hfgpu_fock_build_device(hfgpu_handle* h, double* f_dev, const double* p_dev, double thr_diag,
                             double thr_non_diag, double fp32_cutoff);
 
+/* Device-pointer forms of the cycle-1 calls (direct_hartreefock.f90:102-103):
+ * f_dev += G_diag(p_dev) with the Schwarz pass (fock_build_initial_diag.f90),
+ * and f_dev += G_non_diag(p_dev) alone (fock_build_non_diag.f90; FP32 below
+ * fp32_cutoff when > 0).  nb x nb column-major device arrays; the initial
+ * form synchronises the handle's stream to sort the Schwarz factors. */
+int hfgpu_fock_build_initial_diag_device(hfgpu_handle* h, double* f_dev, const double* p_dev, double thr);
+int hfgpu_fock_build_non_diag_device(hfgpu_handle* h, double* f_dev, const double* p_dev, double thr,
+                                     double fp32_cutoff);
+
 /* Batching form: the whole device build above recorded once as a CUDA graph
  * and replayed with one launch per build.  The 46 per-class loops of
  * fock_build_non_diag.f90 (and the diagonal builders) become one graph of

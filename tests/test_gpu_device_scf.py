@@ -43,3 +43,86 @@ def test_device_scf_mixed_precision():
     fb.close()
     assert r.converged
     assert abs(r.energy - gold["energy"]) < 1e-6
+
+
+# --- the C++ device step (include/hfgpu_scf.h) -------------------------------
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,sysname", [("water", "water"), ("alkane1", "alkane1"), ("benzene", "benzene"),
+                                          ("water_sp", "water_sp"), ("c20h42", "alkane20"), ("c60", "c60")])
+def test_cpp_device_scf_matches_golden(name, sysname):
+    """Every cycle on the device from the library's C++ (cuSOLVER syevd as
+    dsyev): the converged energy matches the oracle's (golden) to 1e-8 Eh."""
+    from hfcode_b200 import scf
+    from hfcode_b200.fock import FockBuilder
+    gold = json.load(open(os.path.join(GOLD, "energies.json")))[name]
+    conve, conv = gold.get("conve", 1e-10), gold.get("conv", 1e-7)
+    mol, _, sh, p0 = system(sysname)
+    fb = FockBuilder(sh)
+    r = scf.device_hartreefock(mol, sh, fb, p_guess=p0, conve=conve, conv=conv, maxiter=150)
+    fb.close()
+    assert r.converged
+    assert abs(r.energy - gold["energy"]) < 1e-8, (r.energy, gold["energy"], r.cycles)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,cutoff", [("benzene", 1e-5), ("alkane20", 1e-7)])
+def test_cpp_device_scf_mixed(name, cutoff):
+    """Mixed form in the incremental builds: within 1e-6 Eh of the oracle's
+    FP64 energy."""
+    from hfcode_b200 import scf
+    from hfcode_b200.fock import FockBuilder
+    key = "c20h42" if name == "alkane20" else name
+    gold = json.load(open(os.path.join(GOLD, "energies.json")))[key]
+    mol, _, sh, p0 = system(name)
+    fb = FockBuilder(sh)
+    r = scf.device_hartreefock(mol, sh, fb, p_guess=p0, conve=gold.get("conve", 1e-10), conv=gold.get("conv", 1e-7),
+                               maxiter=150, fp32_cutoff=cutoff)
+    fb.close()
+    assert r.converged
+    assert abs(r.energy - gold["energy"]) < 1e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["water", "benzene"])
+def test_cpp_device_scf_core_guess_with_level_shift(name):
+    """The core-Hamiltonian guess with the level shift on until DIIS starts
+    (direct_hartreefock.f90:61-91, 200-203): against the oracle's SCF run
+    the same way (oracle/oscf.py), 1e-8 Eh."""
+    from hfcode_b200 import scf
+    from hfcode_b200.fock import FockBuilder
+    from oracle import oscf
+    mol, _, sh, _ = system(name)
+    ref = oscf.OracleSCF(mol.charges, mol.coords, mol.nocc, sh).run(p_guess=None, conve=1e-10, conv=1e-7,
+                                                                     maxiter=150, levshft=0.5)
+    fb = FockBuilder(sh)
+    r = scf.device_hartreefock(mol, sh, fb, p_guess=None, conve=1e-10, conv=1e-7, maxiter=150, levshft=0.5)
+    fb.close()
+    assert r.converged and ref["converged"]
+    assert abs(r.energy - ref["energy"]) < 1e-8, (r.energy, ref["energy"])
+
+
+@pytest.mark.gpu
+def test_cpp_device_scf_resumes():
+    """A run stopped after cycle 1 and continued reaches the same energy as
+    one uninterrupted run, and the orbital energies come back ascending."""
+    import numpy as np
+    from hfcode_b200 import onee
+    from hfcode_b200.fock import DeviceSCFJob, FockBuilder
+    mol, _, sh, p0 = system("alkane1")
+    S, T, V = onee.one_electron(mol, sh, gpu=True)
+    out = []
+    for split in (False, True):
+        fb = FockBuilder(sh)
+        job = DeviceSCFJob(fb, mol.nocc, mol.nuclear_repulsion(), S, T + V, p0)
+        if split:
+            first = job.run(maxiter=1, conve=1e-10, conv=1e-7)
+            assert first["cycles"] == 1 and not first["converged"]
+        r = job.run(maxiter=60, conve=1e-10, conv=1e-7)
+        _, _, eigs = job.get()
+        job.close()
+        fb.close()
+        assert r["converged"]
+        assert np.all(np.diff(eigs) >= 0)
+        out.append(r["energy"])
+    assert abs(out[0] - out[1]) < 1e-10
