@@ -52,6 +52,10 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the FP64-vs-mixed SCF study")
     ap.add_argument("--mixed-cutoffs", default="1e-7,1e-5,1e-3")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served-stream study")
+    ap.add_argument("--serve-jobs", type=int, default=1000)
+    ap.add_argument("--serve-rate", type=float, default=12.0, help="Poisson arrival rate of the served stream")
+    ap.add_argument("--serve-plain", type=int, default=100, help="jobs of the one-at-a-time comparison")
     ap.add_argument("--cutoff", type=float, default=0.0,
                     help="FP32 cutoff of the timed build (0 = the FP64 build the metric is quoted on)")
     return ap.parse_args()
@@ -184,12 +188,21 @@ def cpu_oracle_builds(sh, p, warmup: int, steps: int, stride: int, calibrate: bo
 
 
 def mixed_study(fock, mol, sh, cutoffs, dev):
-    """FP64 vs mixed precision on the SCF path: converged energies of the
-    reference protocol (conve 1e-9) with FP64 and with mixed incremental
-    builds, and the speed of one incremental (delta-P) build near
-    convergence in both forms, with max|dF| between them."""
+    """FP64 vs mixed precision on the SCF path.
+
+    * converged energies of the reference protocol (conve 1e-9) with FP64 and
+      with mixed incremental builds, |dE| against the FP64 run and against
+      the oracle's FP64 energy (golden fixture);
+    * the speed of one incremental (delta-P) build near convergence in both
+      forms, with max|dF| between them;
+    * the whole SCF with the job's state on the device (the library's C++
+      step), FP64 and mixed alternating three times each;
+    * one full build at the converged density;
+    * n-C20H42 (the configuration the mixed target is quoted on) at cutoff
+      1e-7: its incremental-build speed-up and |dE| against the oracle."""
     import torch
     from hfcode_b200 import basis, onee, scf
+    gold = json.load(open(os.path.join(ROOT, "tests", "golden", "energies.json")))
     bas = basis.load_basis("6-31G(d)")
     p0 = basis.density_superposition(mol, bas, sh.nb)
     ints = onee.one_electron(mol, sh, gpu=True)
@@ -198,49 +211,37 @@ def mixed_study(fock, mol, sh, cutoffs, dev):
     t0 = time.perf_counter()
     r64 = scf.direct_hartreefock(mol, sh, fb, p_guess=p0, conve=1e-9, conv=1e-6, maxiter=80, ints=ints)
     out["scf_fp64"] = {"energy": r64.energy, "cycles": r64.cycles, "converged": r64.converged,
-                       "seconds": time.perf_counter() - t0}
-    # the same SCF with every cycle on the device (CUDA-graph replays, SP2
-    # density), FP64 and mixed in the incremental builds
-    from hfcode_b200.device_scf import DeviceSCF
-    # one small device SCF first (benzene): it pages in and initialises what
-    # the device step uses (cuBLAS, graph instantiation, torch's kernels), so
-    # that neither timed run below carries those one-time costs
+                       "seconds": time.perf_counter() - t0,
+                       "abs_dE_vs_oracle": abs(r64.energy - gold["c60"]["energy"]) if sh.nb == 840 else None}
+    # the whole SCF on the device (C++ step), after one small warm-up SCF so
+    # that neither form carries the libraries' first-call costs
     from hfcode_b200 import molecules
     wmol = molecules.benzene()
     wsh = basis.spread_basis(wmol, bas)
-    for cut in (0.0, 1e-5):
-        fbw = fock.FockBuilder(wsh)
-        DeviceSCF(wmol, wsh, fbw).run(basis.density_superposition(wmol, bas, wsh.nb), conve=1e-9, conv=1e-6,
-                                      maxiter=80, fp32_cutoff=cut)
-        fbw.close()
-    # the two forms alternate, twice each; the faster run of each is
-    # reported (these host-driven runs vary by tens of percent run to run)
-    for rep in range(2):
+    fbw = fock.FockBuilder(wsh)
+    scf.device_hartreefock(wmol, wsh, fbw, p_guess=basis.density_superposition(wmol, bas, wsh.nb), conve=1e-9,
+                           conv=1e-6, maxiter=80, fp32_cutoff=1e-5)
+    fbw.close()
+    for rep in range(3):
         for label, cut in (("device_scf_fp64", 0.0), ("device_scf_mixed_1e-05", 1e-5)):
             fbd = fock.FockBuilder(sh)
+            torch.cuda.synchronize()
             t1 = time.perf_counter()
-            rd = DeviceSCF(mol, sh, fbd, ints=ints).run(p0, conve=1e-9, conv=1e-6, maxiter=80, fp32_cutoff=cut)
+            rd = scf.device_hartreefock(mol, sh, fbd, p_guess=p0, conve=1e-9, conv=1e-6, maxiter=80,
+                                        fp32_cutoff=cut, ints=ints)
             sec = time.perf_counter() - t1
             fbd.close()
             runs = out.get(label, {}).get("runs_seconds", []) + [sec]
-            out[label] = {"energy": rd.energy, "cycles": rd.cycles, "converged": rd.converged, "seconds": min(runs),
-                          "runs_seconds": runs, "abs_dE_vs_host_fp64": abs(rd.energy - r64.energy),
-                          "scf_builds_per_s": rd.cycles / min(runs)}
-    # a delta-P near convergence: the converged density against the core-free
-    # one-cycle update (P_next - P), the size the incremental builds see late
+            out[label] = {"energy": rd.energy, "cycles": rd.cycles, "converged": rd.converged,
+                          "seconds": float(np.median(runs)), "runs_seconds": runs,
+                          "spread": (max(runs) - min(runs)) / min(runs),
+                          "abs_dE_vs_host_fp64": abs(rd.energy - r64.energy),
+                          "scf_builds_per_s": rd.cycles / float(np.median(runs))}
     nb = sh.nb
-    f = r64.F
-    X = onee.s_minus_half(ints[0])
-    _, C = np.linalg.eigh(X @ f @ X.T)
-    C = X @ C
-    p_next = 2.0 * C[:, :mol.nocc] @ C[:, :mol.nocc].T
-    dp = p_next - r64.P
-    out["delta_p_max"] = float(np.max(np.abs(dp)))
-    P = torch.from_numpy(np.ascontiguousarray(dp)).to(dev)
-    F = torch.zeros((nb, nb), dtype=torch.float64, device=dev)
     stream = torch.cuda.ExternalStream(fb.stream(), device=dev)
+    F = torch.zeros((nb, nb), dtype=torch.float64, device=dev)
 
-    def timed(cut, reps=3):
+    def timed(P, thr_nd, cut, reps=3):
         ts = []
         for _ in range(reps + 1):
             F.zero_()
@@ -248,16 +249,29 @@ def mixed_study(fock, mol, sh, cutoffs, dev):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            fb.fock_build_device(F.data_ptr(), P.data_ptr(), THR, THR * 0.1, cut)
+            fb.fock_build_device(F.data_ptr(), P.data_ptr(), THR, thr_nd, cut)
             e1.record(stream)
             e1.synchronize()
             ts.append(e0.elapsed_time(e1))
         return float(np.median(ts[1:])), F.cpu().numpy().copy(), fb.class_stats()
 
-    t64, f64, st64 = timed(0.0)
+    # a full build at the converged density
+    Pc = torch.from_numpy(np.ascontiguousarray(r64.P)).to(dev)
+    tc, _, stc = timed(Pc, THR, 0.0)
+    out["converged_density_build"] = {"ms": tc, "builds_per_s": 1000.0 / tc,
+                                      "screened_in_quartets": int(stc["pass"].sum())}
+    # a delta-P near convergence: the one-cycle update of the converged density
+    X = onee.s_minus_half(ints[0])
+    _, C = np.linalg.eigh(X @ r64.F @ X.T)
+    C = X @ C
+    p_next = 2.0 * C[:, :mol.nocc] @ C[:, :mol.nocc].T
+    dp = p_next - r64.P
+    out["delta_p_max"] = float(np.max(np.abs(dp)))
+    P = torch.from_numpy(np.ascontiguousarray(dp)).to(dev)
+    t64, f64, _ = timed(P, THR * 0.1, 0.0)
     out["delta_build_ms_fp64"] = t64
     for cut in cutoffs:
-        tm, fm, stm = timed(cut)
+        tm, fm, stm = timed(P, THR * 0.1, cut)
         fbm = fock.FockBuilder(sh)
         t1 = time.perf_counter()
         rm = scf.direct_hartreefock(mol, sh, fbm, p_guess=p0, conve=1e-9, conv=1e-6, maxiter=80, ints=ints,
@@ -270,7 +284,81 @@ def mixed_study(fock, mol, sh, cutoffs, dev):
             "scf_energy": rm.energy, "abs_dE_vs_fp64": abs(rm.energy - r64.energy), "scf_cycles": rm.cycles,
             "converged": rm.converged, "scf_seconds": time.perf_counter() - t1}
     fb.close()
+    out["c20h42_cutoff_1e-07"] = mixed_c20h42(fock, gold["c20h42"], dev)
     return out
+
+
+def mixed_c20h42(fock, gold, dev):
+    """n-C20H42/6-31G(d) with FP32 below bound 1e-7 in the incremental builds:
+    delta-P build speed-up against FP64 and the converged SCF energy against
+    the oracle's FP64 energy."""
+    import torch
+    from hfcode_b200 import basis, molecules, onee, scf
+    mol = molecules.alkane(20)
+    bas = basis.load_basis("6-31G(d)")
+    sh = basis.spread_basis(mol, bas)
+    p0 = basis.density_superposition(mol, bas, sh.nb)
+    ints = onee.one_electron(mol, sh, gpu=True)
+    fb = fock.FockBuilder(sh)
+    r64 = scf.direct_hartreefock(mol, sh, fb, p_guess=p0, conve=1e-9, conv=1e-6, maxiter=80, ints=ints)
+    fbm = fock.FockBuilder(sh)
+    rm = scf.direct_hartreefock(mol, sh, fbm, p_guess=p0, conve=1e-9, conv=1e-6, maxiter=80, ints=ints,
+                                fp32_cutoff=1e-7)
+    fbm.close()
+    X = onee.s_minus_half(ints[0])
+    _, C = np.linalg.eigh(X @ r64.F @ X.T)
+    C = X @ C
+    dp = 2.0 * C[:, :mol.nocc] @ C[:, :mol.nocc].T - r64.P
+    nb = sh.nb
+    P = torch.from_numpy(np.ascontiguousarray(dp)).to(dev)
+    F = torch.zeros((nb, nb), dtype=torch.float64, device=dev)
+    stream = torch.cuda.ExternalStream(fb.stream(), device=dev)
+
+    def timed(cut, reps=5):
+        ts = []
+        for _ in range(reps + 1):
+            F.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fb.fock_build_device(F.data_ptr(), P.data_ptr(), THR, THR * 0.1, cut)
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts[1:])), F.cpu().numpy().copy()
+
+    t64, f64 = timed(0.0)
+    tm, fm = timed(1e-7)
+    fb.close()
+    return {"nb": nb, "delta_build_ms_fp64": t64, "delta_build_ms_mixed": tm, "speedup_vs_fp64": t64 / tm,
+            "max_abs_dF_vs_fp64": float(np.max(np.abs(fm - f64))),
+            "scf_energy_fp64": r64.energy, "scf_energy_mixed": rm.energy,
+            "abs_dE_mixed_vs_oracle": abs(rm.energy - gold["energy"]),
+            "abs_dE_fp64_vs_oracle": abs(r64.energy - gold["energy"])}
+
+
+def served_study(n_jobs: int, rate: float, slots: int, n_plain: int):
+    """The serving form: a seeded Poisson stream of RHF/6-31G(d) jobs
+    (CnH2n+2 n <= 16, (H2O)k k <= 20; mixed precision at cutoff 1e-7) served
+    with continuous batching, every job's state on the device; and the plain
+    per-job GPU form (one job at a time, same protocol) on the first
+    `n_plain` jobs of the same stream arriving at once."""
+    from hfcode_b200 import serve
+    jobs = serve.make_stream(n_jobs, rate)
+    srv = serve.Server(64 << 30, slots, fp32_cutoff=1e-7)
+    served = srv.serve(jobs)
+    plain_jobs = serve.make_stream(n_plain, 0.0)
+    plain = serve.serve_sequential(plain_jobs, serve.Server(64 << 30, 1, fp32_cutoff=1e-7))
+    sat_jobs = serve.make_stream(n_plain, 0.0)
+    sat = serve.Server(64 << 30, slots, fp32_cutoff=1e-7).serve(sat_jobs, realtime=False)
+    pick = ("jobs", "jobs_per_s", "makespan_s", "latency_ms")
+    return {"stream": {"jobs": n_jobs, "poisson_rate_per_s": rate, "slots": slots, "seed": 20261203,
+                       "fp32_cutoff": 1e-7, "state": "device (hfgpu_scf)"},
+            "served": {k: served[k] for k in pick + ("service_ms", "queue_ms", "failed", "not_converged",
+                                                      "peak_active", "peak_hbm_bytes")},
+            "plain_per_job": {k: plain[k] for k in pick},
+            "served_all_at_once": {k: sat[k] for k in pick + ("failed",)}}
 
 
 def run_reference(args):
@@ -424,6 +512,8 @@ def main():
            "clocks": clk.summary()}
     if rank == 0 and world == 1 and not args.no_mixed:
         out["mixed"] = mixed_study(fock, mol, sh, [float(x) for x in args.mixed_cutoffs.split(",")], dev)
+    if rank == 0 and world == 1 and not args.no_serve:
+        out["served"] = served_study(args.serve_jobs, args.serve_rate, 8, args.serve_plain)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_oracle_builds(sh, p, 1, 2, args.cpu_stride, calibrate=True)
     if rank == 0:

@@ -5,7 +5,8 @@
 //   Fock builds        this library (device-pointer entry points of hfgpu.h)
 //   E_elec, DIIS rows  cuBLAS ddot into device scalars
 //   F P S - S P F, X^T R X, X F X^T, C = X C', P = 2 C_occ C_occ^T   cuBLAS dgemm/geam
-//   the dsyev role     cuSOLVER syevd (ascending eigenvalues, vectors in columns)
+//   the density        SP2 purification (cuBLAS dgemm); cuSOLVER syevd where
+//                      eigenvectors are needed (core guess, level shift, orbital energies)
 //   max |R|, max |dP|  one reduction kernel
 //
 // The host reads one small block of scalars per cycle (two dots, the new
@@ -63,6 +64,95 @@ __global__ void k_scale_cols(const double* __restrict__ v, const double* __restr
     out[t] = v[t] / sqrt(w[t / n]);
 }
 
+// Gershgorin discs of a symmetric n x n matrix, one warp per row (read as
+// the column, which is contiguous): lo[i] = a_ii - r_i, hi[i] = a_ii + r_i,
+// r_i = sum_{j != i} |a_ij|
+__global__ void k_gershgorin_rows(const double* __restrict__ a, int n, double* __restrict__ lo,
+                                  double* __restrict__ hi) {
+    const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (i >= n) return;
+    const double* col = a + (size_t)i * n;
+    double r = 0.0;
+    for (int j = lane; j < n; j += 32)
+        if (j != i) r += fabs(col[j]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+    if (lane == 0) {
+        lo[i] = col[i] - r;
+        hi[i] = col[i] + r;
+    }
+}
+
+// bounds[0] = min lo, bounds[1] = max hi (one block of 1024 threads)
+__global__ void k_gershgorin_bounds(const double* __restrict__ lo, const double* __restrict__ hi, int n,
+                                    double* bounds) {
+    __shared__ double slo[1024], shi[1024];
+    double a = 1e300, b = -1e300;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        a = fmin(a, lo[i]);
+        b = fmax(b, hi[i]);
+    }
+    slo[threadIdx.x] = a;
+    shi[threadIdx.x] = b;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            slo[threadIdx.x] = fmin(slo[threadIdx.x], slo[threadIdx.x + o]);
+            shi[threadIdx.x] = fmax(shi[threadIdx.x], shi[threadIdx.x + o]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        bounds[0] = slo[0];
+        bounds[1] = shi[0];
+    }
+}
+
+// X = (hi I - F) / (hi - lo): the start of the purification, spectrum in [0, 1]
+// with the occupied orbitals (lowest energies) nearest 1
+__global__ void k_sp2_start(const double* __restrict__ f, const double* __restrict__ bounds, double* __restrict__ x,
+                            int n) {
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t >= (size_t)n * n) return;
+    const double lo = bounds[0], hi = bounds[1];
+    const int i = (int)(t % n), j = (int)(t / n);
+    x[t] = ((i == j ? hi : 0.0) - f[t]) / (hi - lo);
+}
+
+// traces of X and X^2 into tr[0], tr[1] (one block)
+__global__ void k_traces(const double* __restrict__ x, const double* __restrict__ x2, int n, double* tr) {
+    __shared__ double s1[256], s2[256];
+    double a = 0.0, b = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        a += x[i + (size_t)i * n];
+        b += x2[i + (size_t)i * n];
+    }
+    s1[threadIdx.x] = a;
+    s2[threadIdx.x] = b;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            s1[threadIdx.x] += s1[threadIdx.x + o];
+            s2[threadIdx.x] += s2[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        tr[0] = s1[0];
+        tr[1] = s2[0];
+    }
+}
+
+// One SP2 step: X <- X^2 when that brings the trace nearer nocc, else
+// X <- 2X - X^2 (trace of 2X - X^2 is 2 tr X - tr X^2).
+__global__ void k_sp2_step(double* __restrict__ x, const double* __restrict__ x2, const double* __restrict__ tr,
+                           double nocc, size_t n2) {
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t >= n2) return;
+    const bool square = fabs(tr[1] - nocc) < fabs(2.0 * tr[0] - tr[1] - nocc);
+    x[t] = square ? x2[t] : 2.0 * x[t] - x2[t];
+}
+
 int fail(int code, const std::string& msg) {
     hfgpu::set_last_error(msg);
     return code;
@@ -88,6 +178,8 @@ struct hfgpu_scf {
     int* info = nullptr;
     void* blas_ws = nullptr;
     CycleScalars* sc = nullptr;  // device
+    double* aux = nullptr;       // purification: bounds[2], traces[2], then row bounds lo[nb], hi[nb]
+    bool eigs_current = false;   // W/eigs describe the last Fob
     size_t bytes = 0;
     // protocol state, carried from one hfgpu_scf_run call to the next
     double eelec = 0.0;
@@ -166,6 +258,44 @@ int density_from_cob(hfgpu_scf* s, double* P) {
     return HFGPU_OK;
 }
 
+// P = 2 X D X^T from the orthogonalised Fock matrix Fo by second-order
+// spectral projection (A. M. N. Niklasson, Phys. Rev. B 66, 155115 (2002)):
+// D is the projector on the nocc lowest eigenvectors of Fo, the density the
+// eigenvectors give (direct_hartreefock.f90:204-218), reached with matrix
+// products only.  Each step's choice is made on the device; the host checks
+// idempotency every few steps.
+int density_by_purification(hfgpu_scf* s, const double* Fo, double* P) {
+    const int nb = s->nb;
+    const size_t n2 = (size_t)nb * nb;
+    const unsigned blocks = (unsigned)((n2 + 255) / 256);
+    double* X = s->T1;
+    double* X2 = s->T2;
+    double* bounds = s->aux;
+    double* tr = s->aux + 2;
+    k_gershgorin_rows<<<(unsigned)((nb + 7) / 8), 256, 0, s->st>>>(Fo, nb, s->aux + 4, s->aux + 4 + nb);
+    k_gershgorin_bounds<<<1, 1024, 0, s->st>>>(s->aux + 4, s->aux + 4 + nb, nb, bounds);
+    k_sp2_start<<<blocks, 256, 0, s->st>>>(Fo, bounds, X, nb);
+    SCF_CUDA(cudaGetLastError());
+    constexpr int BLOCK = 8, MAXSTEP = 160;
+    for (int step = 0; step < MAXSTEP; step += BLOCK) {
+        for (int k = 0; k < BLOCK; ++k) {
+            SCF_RC(gemm(s, false, false, 1.0, X, X, 0.0, X2));
+            k_traces<<<1, 256, 0, s->st>>>(X, X2, nb, tr);
+            k_sp2_step<<<blocks, 256, 0, s->st>>>(X, X2, tr, (double)s->nocc, n2);
+        }
+        SCF_CUDA(cudaGetLastError());
+        double h_tr[2];
+        SCF_CUDA(cudaMemcpyAsync(h_tr, tr, sizeof(h_tr), cudaMemcpyDeviceToHost, s->st));
+        SCF_CUDA(cudaStreamSynchronize(s->st));
+        // tr X - tr X^2 = sum x_k (1 - x_k) over the eigenvalues: zero for a projector
+        if (std::fabs(h_tr[0] - h_tr[1]) < 1e-11 * std::max(1, s->nocc)) break;
+    }
+    // P = 2 X_s D X_s^T with X_s = S^-1/2
+    SCF_RC(gemm(s, false, false, 1.0, s->X, X, 0.0, X2));
+    SCF_RC(gemm(s, false, true, 2.0, X2, s->X, 0.0, P));
+    return HFGPU_OK;
+}
+
 // Solves the bordered DIIS system A x = b in place (Gaussian elimination
 // with partial pivoting; dsysv's role, wrapper_dsygv.f90:55-78).
 bool small_solve(std::vector<double>& A, std::vector<double>& b, int n) {
@@ -205,6 +335,7 @@ void release(hfgpu_scf* s) {
     }
     if (s->info) cudaFree(s->info);
     if (s->sc) cudaFree(s->sc);
+    if (s->aux) cudaFree(s->aux);
     if (s->blas_ws) cudaFree(s->blas_ws);
     if (s->blas) cublasDestroy(s->blas);
     if (s->sol) cusolverDnDestroy(s->sol);
@@ -234,6 +365,7 @@ int create(hfgpu_handle* h, int nocc, double enuc, const double* S, const double
         SCF_CUDA(cudaMalloc((void**)&s->W, nb * sizeof(double)));
         SCF_CUDA(cudaMalloc((void**)&s->info, sizeof(int)));
         SCF_CUDA(cudaMalloc((void**)&s->sc, sizeof(CycleScalars)));
+        SCF_CUDA(cudaMalloc((void**)&s->aux, (4 + 2 * (size_t)nb) * sizeof(double)));
         SCF_BLAS(cublasCreate(&s->blas));
         SCF_BLAS(cublasSetStream(s->blas, s->st));
         const size_t ws = 4u << 20;  // cuBLAS gets its workspace here, so it never allocates later
@@ -245,7 +377,7 @@ int create(hfgpu_handle* h, int nocc, double enuc, const double* S, const double
                                                nb, s->W, &s->lwork));
         SCF_CUDA(cudaMalloc((void**)&s->work, (size_t)std::max(1, s->lwork) * sizeof(double)));
         s->bytes = (13 + 2 * NDIIS) * bytes + nb * sizeof(double) + ws + (size_t)s->lwork * sizeof(double) +
-                   sizeof(CycleScalars) + sizeof(int);
+                   sizeof(CycleScalars) + sizeof(int) + (4 + 2 * (size_t)nb) * sizeof(double);
     }
     SCF_CUDA(cudaMemcpyAsync(s->S, S, bytes, cudaMemcpyHostToDevice, s->st));
     SCF_CUDA(cudaMemcpyAsync(s->H, hcore, bytes, cudaMemcpyHostToDevice, s->st));
@@ -421,14 +553,20 @@ int run(hfgpu_scf* s, const hfgpu_scf_params& prm, hfgpu_scf_result* res) {
                                  s->Cob + (size_t)s->nocc * nb, nb, s->Cob + (size_t)s->nocc * nb, nb, &one, s->Fob,
                                  nb));
         }
-        SCF_RC(eigensolve(s, s->Fob));  // :204-205
+        // :204-205.  The eigenvectors are needed only while the level shift
+        // acts on them; otherwise the density comes from purification and the
+        // orbital energies are left for hfgpu_scf_get
+        const bool vectors = s->uselevshft && prm.levshft > 0.0;
+        if (vectors) SCF_RC(eigensolve(s, s->Fob));
+        s->eigs_current = vectors;
         s->eelec = eelec;
         if (std::fabs(deltae) < prm.conve && deltap < prm.conv && it > 1) {  // :211-216
             converged = true;
             break;
         }
         SCF_RC(copy(s, s->Pold, s->P));
-        SCF_RC(density_from_cob(s, s->P));
+        if (vectors) SCF_RC(density_from_cob(s, s->P));
+        else SCF_RC(density_by_purification(s, s->Fob, s->P));
     }
     SCF_CUDA(cudaStreamSynchronize(s->st));
     if (res) {
@@ -482,9 +620,14 @@ int hfgpu_scf_run(hfgpu_scf* s, const hfgpu_scf_params* prm, hfgpu_scf_result* r
     return run(s, p, res);
 }
 
-int hfgpu_scf_get(const hfgpu_scf* s, double* p, double* f, double* eigs) {
+int hfgpu_scf_get(hfgpu_scf* s, double* p, double* f, double* eigs) {
     if (!s) return fail(HFGPU_ERR_ARG, "hfgpu_scf_get: null job");
     const size_t bytes = (size_t)s->nb * s->nb * sizeof(double);
+    if (eigs && !s->eigs_current) {  // the last cycle's eigensolve, done on request
+        int rc = eigensolve(s, s->Fob);
+        if (rc) return rc;
+        s->eigs_current = true;
+    }
     if (p) SCF_CUDA(cudaMemcpyAsync(p, s->P, bytes, cudaMemcpyDeviceToHost, s->st));
     if (f) SCF_CUDA(cudaMemcpyAsync(f, s->Fprev, bytes, cudaMemcpyDeviceToHost, s->st));
     SCF_CUDA(cudaStreamSynchronize(s->st));

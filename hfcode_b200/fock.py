@@ -319,7 +319,7 @@ class DeviceSCFJob:
         return {k: getattr(res, k) for k, _ in ScfResult._fields_}
 
     def get(self):
-        """(P, F, orbital energies) as host arrays."""
+        """(P, F, orbital energies of the last cycle) as host arrays."""
         p, f, e = np.zeros((self.nb, self.nb)), np.zeros((self.nb, self.nb)), np.zeros(self.nb)
         _check(_lib.hfgpu_scf_get(self.s, _dp(p), _dp(f), _dp(e)), "scf_get")
         return p, f, e

@@ -8,10 +8,14 @@
  * whole state -- density, Fock matrices, DIIS histories, S^-1/2, core
  * Hamiltonian and the builder's screening tables -- stays in the GPU's
  * memory, and the cycle runs from C++ on the builder handle's stream:
- * the Fock builds of this library, cuBLAS products and cuSOLVER's syevd in
- * the role of dsyev (eigenvalues ascending, eigenvectors in columns).  Only a
- * few scalars per cycle come back to the host, where the protocol's
- * decisions are taken as the reference takes them.
+ * the Fock builds of this library and cuBLAS products.  The reference's
+ * eigensolve gives the new density from the nocc lowest eigenvectors of the
+ * orthogonalised Fock matrix; here that projector is formed by second-order
+ * spectral projection (SP2, matrix products only), and cuSOLVER's syevd
+ * (dsyev's role) runs only where eigenvectors are needed: the
+ * core-Hamiltonian guess, cycles with the level shift on, and the orbital
+ * energies on request.  A few scalars per cycle come back to the host, where
+ * the protocol's decisions are taken as the reference takes them.
  *
  * One job per builder handle (the job uses the handle's stream); jobs on
  * different handles run concurrently from different host threads.
@@ -71,8 +75,10 @@ int hfgpu_scf_create(hfgpu_handle* h, int nocc, double enuc, const double* S, co
 int hfgpu_scf_run(hfgpu_scf* s, const hfgpu_scf_params* prm, hfgpu_scf_result* res);
 
 /* Host copies of the current density, of the last Fock matrix (the
- * reference's faobold) and of the orbital energies (nb values, ascending). */
-int hfgpu_scf_get(const hfgpu_scf* s, double* p, double* f, double* eigs);
+ * reference's faobold) and of the last cycle's orbital energies (nb values,
+ * ascending; solved on request when the cycle did not need eigenvectors).
+ * Any pointer may be NULL. */
+int hfgpu_scf_get(hfgpu_scf* s, double* p, double* f, double* eigs);
 
 /* Device memory held by the job (not counting the builder handle). */
 int hfgpu_scf_device_bytes(const hfgpu_scf* s, size_t* bytes);
