@@ -372,15 +372,26 @@ int set_err(int code, const std::string& msg) {
     return code;
 }
 
+// Device buffers of a handle come from the stream-ordered allocator on the
+// handle's stream: cudaFreeAsync, unlike cudaFree, does not synchronise the
+// whole device, so a served job that finishes does not stall the jobs still
+// running on the GPU.
 template <typename T>
-int dalloc(T** p, size_t n) {
+int dalloc(T** p, size_t n, cudaStream_t st) {
     if (n == 0) n = 1;
-    cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+    cudaError_t e = cudaMallocAsync((void**)p, n * sizeof(T), st);
     if (e != cudaSuccess) {
-        g_err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+        *p = nullptr;
+        g_err = std::string("cudaMallocAsync: ") + cudaGetErrorString(e);
         return HFGPU_ERR_NOMEM;
     }
     return HFGPU_OK;
+}
+
+template <typename T>
+void dfree(T*& p, cudaStream_t st) {
+    if (p) cudaFreeAsync((void*)p, st);
+    p = nullptr;
 }
 
 // class index of pair types (i <= j) in the generator's class order
@@ -610,9 +621,8 @@ int build_active(hfgpu_handle* h) {
     }
     {
         std::vector<double> soa = prims_soa(aprims);
-        if (h->d_apsoa) cudaFree(h->d_apsoa);
-        h->d_apsoa = nullptr;
-        int rc = dalloc(&h->d_apsoa, std::max<size_t>(soa.size(), 1));
+        dfree(h->d_apsoa, h->stream);
+        int rc = dalloc(&h->d_apsoa, std::max<size_t>(soa.size(), 1), h->stream);
         if (rc) return rc;
         h->apsoa = soa_view(h->d_apsoa, aprims.size());
         h->naprims = aprims.size();
@@ -674,14 +684,12 @@ int build_active(hfgpu_handle* h) {
     h->ntot = start;
     total_q = qoff;
     if (h->hsubs.size() > h->subcap) {
-        if (h->d_subs) cudaFree(h->d_subs);
-        h->d_subs = nullptr;
+        dfree(h->d_subs, h->stream);
         h->subcap = 0;
-        int rc = dalloc(&h->d_subs, h->hsubs.size());
+        int rc = dalloc(&h->d_subs, h->hsubs.size(), h->stream);
         if (rc) return rc;
-        if (h->d_cnt) cudaFree(h->d_cnt);
-        h->d_cnt = nullptr;
-        rc = dalloc(&h->d_cnt, 2 * h->hsubs.size());
+        dfree(h->d_cnt, h->stream);
+        rc = dalloc(&h->d_cnt, 2 * h->hsubs.size(), h->stream);
         if (rc) return rc;
         h->subcap = h->hsubs.size();
     }
@@ -692,10 +700,9 @@ int build_active(hfgpu_handle* h) {
         HF_CHECK(cudaStreamSynchronize(h->stream));
     }
     if ((size_t)total_q > h->qcap) {
-        if (h->d_q) cudaFree(h->d_q);
-        h->d_q = nullptr;
+        dfree(h->d_q, h->stream);
         h->qcap = 0;
-        int rc = dalloc(&h->d_q, (size_t)total_q);
+        int rc = dalloc(&h->d_q, (size_t)total_q, h->stream);
         if (rc) return rc;
         h->qcap = (size_t)std::max<long long>(total_q, 1);
     }
@@ -715,10 +722,9 @@ int build_active(hfgpu_handle* h) {
         need = std::max(need, st * per);
     }
     if (need * NSTREAM > h->scratch_doubles) {
-        if (h->d_scratch) cudaFree(h->d_scratch);
-        h->d_scratch = nullptr;
+        dfree(h->d_scratch, h->stream);
         h->scratch_doubles = 0;
-        int rc = dalloc(&h->d_scratch, need * NSTREAM);
+        int rc = dalloc(&h->d_scratch, need * NSTREAM, h->stream);
         if (rc) return rc;
         h->scratch_doubles = need * NSTREAM;
     }
@@ -966,33 +972,41 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
     }
     int rc = 0;
     const size_t nb2 = (size_t)h->nb * h->nb;
-    rc |= dalloc(&h->d_shtyp, h->nsh);
-    rc |= dalloc(&h->d_aosh, h->nsh);
-    rc |= dalloc(&h->d_psoa, 8 * std::max<size_t>(prims.size(), 1));
-    rc |= dalloc(&h->d_boys, bt.size());
-    rc |= dalloc(&h->d_boysf, btf.size());
-    rc |= dalloc(&h->d_P, nb2);
-    rc |= dalloc(&h->d_F, nb2);
-    rc |= dalloc(&h->d_G, nb2);
-    rc |= dalloc(&h->d_md, (size_t)h->nsh * h->nsh);
-    rc |= dalloc(&h->d_cnt, 2 * NCLS);
-    rc |= dalloc(&h->d_stats, NCLS);
-    rc |= dalloc(&h->d_ncls, 2 * NCLS);
-    rc |= dalloc(&h->d_Pb, nb2);
-    rc |= dalloc(&h->d_boff, (size_t)h->nsh * h->nsh);
-    rc |= dalloc(&h->d_aomap, (size_t)h->nb);
-    rc |= dalloc(&h->d_nfsh, (size_t)h->nsh);
+    rc |= dalloc(&h->d_shtyp, h->nsh, h->stream);
+    rc |= dalloc(&h->d_aosh, h->nsh, h->stream);
+    rc |= dalloc(&h->d_psoa, 8 * std::max<size_t>(prims.size(), 1), h->stream);
+    rc |= dalloc(&h->d_boys, bt.size(), h->stream);
+    rc |= dalloc(&h->d_boysf, btf.size(), h->stream);
+    rc |= dalloc(&h->d_P, nb2, h->stream);
+    rc |= dalloc(&h->d_F, nb2, h->stream);
+    rc |= dalloc(&h->d_G, nb2, h->stream);
+    rc |= dalloc(&h->d_md, (size_t)h->nsh * h->nsh, h->stream);
+    rc |= dalloc(&h->d_cnt, 2 * NCLS, h->stream);
+    rc |= dalloc(&h->d_stats, NCLS, h->stream);
+    rc |= dalloc(&h->d_ncls, 2 * NCLS, h->stream);
+    rc |= dalloc(&h->d_Pb, nb2, h->stream);
+    rc |= dalloc(&h->d_boff, (size_t)h->nsh * h->nsh, h->stream);
+    rc |= dalloc(&h->d_aomap, (size_t)h->nb, h->stream);
+    rc |= dalloc(&h->d_nfsh, (size_t)h->nsh, h->stream);
     for (int t = 0; t < NPT; ++t) {
         size_t n = h->pairs[t].size();
-        rc |= dalloc(&h->d_pairs[t], n);
-        rc |= dalloc(&h->d_schw[t], n);
-        rc |= dalloc(&h->d_apairs[t], n);
-        rc |= dalloc(&h->d_ash[t], n);
-        rc |= dalloc(&h->d_aschw[t], n);
+        rc |= dalloc(&h->d_pairs[t], n, h->stream);
+        rc |= dalloc(&h->d_schw[t], n, h->stream);
+        rc |= dalloc(&h->d_apairs[t], n, h->stream);
+        rc |= dalloc(&h->d_ash[t], n, h->stream);
+        rc |= dalloc(&h->d_aschw[t], n, h->stream);
     }
     if (rc) {
         hfgpu_finalize(h);
         return HFGPU_ERR_NOMEM;
+    }
+    // the buffers are ready for the synchronous uploads below once the
+    // handle's stream has run the allocations
+    ce = cudaStreamSynchronize(h->stream);
+    if (ce != cudaSuccess) {
+        std::string m = std::string("hfgpu_init: ") + cudaGetErrorString(ce);
+        hfgpu_finalize(h);
+        return set_err(HFGPU_ERR_CUDA, m);
     }
     for (int i = 0; i < 2 * NCLS + 2; ++i) cudaEventCreate(&h->ev[i]);
     cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming);
@@ -1052,16 +1066,17 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
             if (K.mode == 0 || n == 0) continue;
             std::vector<uint2> dl(n);
             for (size_t i = 0; i < n; ++i) dl[i] = make_uint2((unsigned)i, (unsigned)i);
-            if (dalloc(&h->d_diaglist[t], n)) {
+            if (dalloc(&h->d_diaglist[t], n, h->stream)) {
                 hfgpu_finalize(h);
                 return HFGPU_ERR_NOMEM;
             }
-            ce = up(h->d_diaglist[t], dl.data(), n * sizeof(uint2));
+            ce = cudaMemcpyAsync(h->d_diaglist[t], dl.data(), n * sizeof(uint2), cudaMemcpyHostToDevice, h->stream);
         }
     }
-    if (ce == cudaSuccess) ce = cudaMemset(h->d_stats, 0, NCLS * sizeof(ClassStats));
-    if (ce == cudaSuccess) ce = cudaMemset(h->d_ncls, 0, 2 * NCLS * sizeof(unsigned long long));
-    if (ce == cudaSuccess) ce = cudaDeviceSynchronize();
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(h->d_stats, 0, NCLS * sizeof(ClassStats), h->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(h->d_ncls, 0, 2 * NCLS * sizeof(unsigned long long), h->stream);
+    // the handle's own stream only: other handles' work on the device goes on
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->stream);
     if (ce != cudaSuccess) {
         std::string m = std::string("hfgpu_init: ") + cudaGetErrorString(ce);
         hfgpu_finalize(h);
@@ -1081,11 +1096,11 @@ int hfgpu_finalize(hfgpu_handle* h) {
                     h->d_md, h->d_subs, h->d_q, h->d_cnt, h->d_stats, h->d_scratch, h->d_dscratch,
                     h->d_ncls, h->d_Pb, h->d_boff, h->d_aomap, h->d_nfsh};
     for (void* b : bufs)
-        if (b) cudaFree(b);
+        if (b) cudaFreeAsync(b, h->stream);
     for (int t = 0; t < NPT; ++t) {
         void* tb[] = {h->d_pairs[t], h->d_schw[t], h->d_apairs[t], h->d_ash[t], h->d_aschw[t], h->d_diaglist[t]};
         for (void* b : tb)
-            if (b) cudaFree(b);
+            if (b) cudaFreeAsync(b, h->stream);
     }
     for (int i = 0; i < 2 * NCLS + 2; ++i)
         if (h->ev[i]) cudaEventDestroy(h->ev[i]);
@@ -1097,7 +1112,10 @@ int hfgpu_finalize(hfgpu_handle* h) {
         if (h->join[k]) cudaEventDestroy(h->join[k]);
     }
     if (h->fork) cudaEventDestroy(h->fork);
-    if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->stream) {
+        cudaStreamSynchronize(h->stream);  // the stream-ordered frees above
+        cudaStreamDestroy(h->stream);
+    }
     delete h;
     return HFGPU_OK;
 }
@@ -1119,7 +1137,7 @@ static int alloc_diag_scratch(hfgpu_handle* h) {
         need = std::max(need, st * per);
     }
     if (!need) return HFGPU_OK;
-    const int rc = dalloc(&h->d_dscratch, need);
+    const int rc = dalloc(&h->d_dscratch, need, h->stream);
     if (rc == HFGPU_OK) h->dscratch_doubles = need;
     return rc;
 }

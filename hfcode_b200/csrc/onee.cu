@@ -457,14 +457,18 @@ thread_local std::string g_onee_err;
 
 namespace hfgpu {
 void set_last_error(const std::string& msg);  // hfgpu.cu
-std::recursive_mutex& device_mutex();         // hfgpu.cu: serialises allocations against captures
 }
 
 namespace {
+// Stream-ordered allocation and upload on the call's own stream: no
+// device-wide synchronisation, so calls of concurrent jobs (and a capture in
+// another thread) go on undisturbed.  Pageable sources are staged by the
+// copy before it returns.
 template <typename T>
-cudaError_t up(T** d, const std::vector<T>& h) {
-    cudaError_t e = cudaMalloc((void**)d, std::max<size_t>(h.size(), 1) * sizeof(T));
-    if (e == cudaSuccess && !h.empty()) e = cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+cudaError_t up(T** d, const std::vector<T>& h, cudaStream_t st) {
+    cudaError_t e = cudaMallocAsync((void**)d, std::max<size_t>(h.size(), 1) * sizeof(T), st);
+    if (e == cudaSuccess && !h.empty())
+        e = cudaMemcpyAsync(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st);
     return e;
 }
 }  // namespace
@@ -476,7 +480,6 @@ extern "C" int hfgpu_one_electron_gpu(const hfgpu_basis* B, int natom, const dou
         return HFGPU_ERR_ARG;
     }
     const int nb = B->nb, nsh = B->nsh, MP = B->maxprim;
-    std::lock_guard<std::recursive_mutex> lk(hfgpu::device_mutex());
     // one recursion plan per pair of shell types
     std::map<std::pair<int, int>, int> clsid;
     std::vector<OneeClass> cls;
@@ -552,22 +555,28 @@ extern "C" int hfgpu_one_electron_gpu(const hfgpu_basis* B, int natom, const dou
     NucOp* d_ops = nullptr;
     double *d_xsh = nullptr, *d_zeta = nullptr, *d_djk = nullptr, *d_djkl = nullptr, *d_ch = nullptr,
            *d_xyz = nullptr, *d_out = nullptr;
-    cudaError_t e = up(&d_pairs, sp);
-    if (e == cudaSuccess) e = up(&d_pcls, sc);
-    if (e == cudaSuccess) e = up(&d_cls, cls);
-    if (e == cudaSuccess) e = up(&d_ops, ops);
-    if (e == cudaSuccess) e = up(&d_targets, targets);
-    if (e == cudaSuccess) e = up(&d_shtyp, shtyp);
-    if (e == cudaSuccess) e = up(&d_nzet, nzet);
-    if (e == cudaSuccess) e = up(&d_aosh, aosh);
-    if (e == cudaSuccess) e = up(&d_xsh, xsh);
-    if (e == cudaSuccess) e = up(&d_zeta, zeta);
-    if (e == cudaSuccess) e = up(&d_djk, djk);
-    if (e == cudaSuccess) e = up(&d_djkl, djkl);
-    if (e == cudaSuccess) e = up(&d_ch, ch);
-    if (e == cudaSuccess) e = up(&d_xyz, xz);
+    cudaStream_t st = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        hfgpu::set_last_error(std::string("hfgpu_one_electron_gpu: ") + cudaGetErrorString(e));
+        return HFGPU_ERR_CUDA;
+    }
+    e = up(&d_pairs, sp, st);
+    if (e == cudaSuccess) e = up(&d_pcls, sc, st);
+    if (e == cudaSuccess) e = up(&d_cls, cls, st);
+    if (e == cudaSuccess) e = up(&d_ops, ops, st);
+    if (e == cudaSuccess) e = up(&d_targets, targets, st);
+    if (e == cudaSuccess) e = up(&d_shtyp, shtyp, st);
+    if (e == cudaSuccess) e = up(&d_nzet, nzet, st);
+    if (e == cudaSuccess) e = up(&d_aosh, aosh, st);
+    if (e == cudaSuccess) e = up(&d_xsh, xsh, st);
+    if (e == cudaSuccess) e = up(&d_zeta, zeta, st);
+    if (e == cudaSuccess) e = up(&d_djk, djk, st);
+    if (e == cudaSuccess) e = up(&d_djkl, djkl, st);
+    if (e == cudaSuccess) e = up(&d_ch, ch, st);
+    if (e == cudaSuccess) e = up(&d_xyz, xz, st);
     const size_t nb2 = (size_t)nb * nb;
-    if (e == cudaSuccess) e = cudaMalloc((void**)&d_out, 3 * nb2 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_out, 3 * nb2 * sizeof(double), st);
     if (e == cudaSuccess) {
         g.pairs = d_pairs; g.pcls = d_pcls; g.npairs = (int)sp.size(); g.cls = d_cls; g.ops = d_ops;
         g.targets = d_targets; g.shtyp = d_shtyp; g.nzet = d_nzet; g.aosh = d_aosh; g.xsh = d_xsh;
@@ -576,17 +585,21 @@ extern "C" int hfgpu_one_electron_gpu(const hfgpu_basis* B, int natom, const dou
         g.S = S ? d_out : nullptr;
         g.T = T ? d_out + nb2 : nullptr;
         g.V = V ? d_out + 2 * nb2 : nullptr;
-        k_onee<<<(g.npairs + 127) / 128, 128>>>(g);
+        k_onee<<<(g.npairs + 127) / 128, 128, 0, st>>>(g);
         e = cudaGetLastError();
     }
-    if (e == cudaSuccess) e = cudaDeviceSynchronize();
-    if (e == cudaSuccess && S) e = cudaMemcpy(S, d_out, nb2 * sizeof(double), cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess && T) e = cudaMemcpy(T, d_out + nb2, nb2 * sizeof(double), cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess && V) e = cudaMemcpy(V, d_out + 2 * nb2, nb2 * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && S) e = cudaMemcpyAsync(S, d_out, nb2 * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && T)
+        e = cudaMemcpyAsync(T, d_out + nb2, nb2 * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && V)
+        e = cudaMemcpyAsync(V, d_out + 2 * nb2, nb2 * sizeof(double), cudaMemcpyDeviceToHost, st);
     void* bufs[] = {d_pairs, d_pcls, d_cls, d_ops, d_targets, d_shtyp, d_nzet, d_aosh, d_xsh, d_zeta, d_djk,
                     d_djkl, d_ch, d_xyz, d_out};
     for (void* b : bufs)
-        if (b) cudaFree(b);
+        if (b) cudaFreeAsync(b, st);
+    const cudaError_t es = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = es;
+    cudaStreamDestroy(st);
     if (e != cudaSuccess) {
         hfgpu::set_last_error(std::string("hfgpu_one_electron_gpu: ") + cudaGetErrorString(e));
         return HFGPU_ERR_CUDA;

@@ -177,6 +177,7 @@ struct hfgpu_scf {
     int lwork = 0;
     int* info = nullptr;
     void* blas_ws = nullptr;
+    void* arena = nullptr;       // one stream-ordered allocation holding every buffer above
     CycleScalars* sc = nullptr;  // device
     double* aux = nullptr;       // purification: bounds[2], traces[2], then row bounds lo[nb], hi[nb]
     bool eigs_current = false;   // W/eigs describe the last Fob
@@ -322,23 +323,47 @@ bool small_solve(std::vector<double>& A, std::vector<double>& b, int n) {
     return true;
 }
 
-void release(hfgpu_scf* s) {
-    std::lock_guard<std::recursive_mutex> lk(hfgpu::device_mutex());
-    if (s->st) cudaStreamSynchronize(s->st);
-    double* bufs[] = {s->S, s->H, s->X, s->P, s->Pold, s->F, s->Fprev, s->dP, s->dF, s->T1, s->T2, s->Fob, s->Cob,
-                      s->W, s->work};
-    for (double* b : bufs)
-        if (b) cudaFree(b);
-    for (int k = 0; k < NDIIS; ++k) {
-        if (s->R[k]) cudaFree(s->R[k]);
-        if (s->FO[k]) cudaFree(s->FO[k]);
+// cuBLAS / cuSOLVER handles are pooled across jobs: creating them costs
+// milliseconds and may allocate, so a served job borrows a pair and gives it
+// back when it ends.
+struct LinAlg {
+    cublasHandle_t blas;
+    cusolverDnHandle_t sol;
+};
+std::mutex g_pool_mu;
+std::vector<LinAlg> g_pool;
+
+int acquire_linalg(hfgpu_scf* s) {
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        if (!g_pool.empty()) {
+            s->blas = g_pool.back().blas;
+            s->sol = g_pool.back().sol;
+            g_pool.pop_back();
+        }
     }
-    if (s->info) cudaFree(s->info);
-    if (s->sc) cudaFree(s->sc);
-    if (s->aux) cudaFree(s->aux);
-    if (s->blas_ws) cudaFree(s->blas_ws);
-    if (s->blas) cublasDestroy(s->blas);
-    if (s->sol) cusolverDnDestroy(s->sol);
+    if (!s->blas) {
+        std::lock_guard<std::recursive_mutex> lk(hfgpu::device_mutex());  // creation may allocate
+        SCF_BLAS(cublasCreate(&s->blas));
+        SCF_SOLVER(cusolverDnCreate(&s->sol));
+    }
+    SCF_BLAS(cublasSetStream(s->blas, s->st));
+    SCF_BLAS(cublasSetPointerMode(s->blas, CUBLAS_POINTER_MODE_HOST));
+    SCF_SOLVER(cusolverDnSetStream(s->sol, s->st));
+    return HFGPU_OK;
+}
+
+void release(hfgpu_scf* s) {
+    if (s->st) cudaStreamSynchronize(s->st);
+    if (s->arena) cudaFreeAsync(s->arena, s->st);
+    if (s->st) cudaStreamSynchronize(s->st);
+    if (s->blas && s->sol) {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        g_pool.push_back({s->blas, s->sol});
+    } else {
+        if (s->blas) cublasDestroy(s->blas);
+        if (s->sol) cusolverDnDestroy(s->sol);
+    }
     delete s;
 }
 
@@ -353,32 +378,43 @@ int create(hfgpu_handle* h, int nocc, double enuc, const double* S, const double
     s->enuc = enuc;
     s->st = (cudaStream_t)hfgpu_stream(h);
     const size_t n2 = (size_t)nb * nb, bytes = n2 * sizeof(double);
-    {
-        std::lock_guard<std::recursive_mutex> lk(hfgpu::device_mutex());  // no allocation during a capture
-        double** mats[] = {&s->S, &s->H, &s->X, &s->P, &s->Pold, &s->F, &s->Fprev, &s->dP, &s->dF, &s->T1, &s->T2,
-                           &s->Fob, &s->Cob};
-        for (double** m : mats) SCF_CUDA(cudaMalloc((void**)m, bytes));
-        for (int k = 0; k < NDIIS; ++k) {
-            SCF_CUDA(cudaMalloc((void**)&s->R[k], bytes));
-            SCF_CUDA(cudaMalloc((void**)&s->FO[k], bytes));
-        }
-        SCF_CUDA(cudaMalloc((void**)&s->W, nb * sizeof(double)));
-        SCF_CUDA(cudaMalloc((void**)&s->info, sizeof(int)));
-        SCF_CUDA(cudaMalloc((void**)&s->sc, sizeof(CycleScalars)));
-        SCF_CUDA(cudaMalloc((void**)&s->aux, (4 + 2 * (size_t)nb) * sizeof(double)));
-        SCF_BLAS(cublasCreate(&s->blas));
-        SCF_BLAS(cublasSetStream(s->blas, s->st));
-        const size_t ws = 4u << 20;  // cuBLAS gets its workspace here, so it never allocates later
-        SCF_CUDA(cudaMalloc(&s->blas_ws, ws));
-        SCF_BLAS(cublasSetWorkspace(s->blas, s->blas_ws, ws));
-        SCF_SOLVER(cusolverDnCreate(&s->sol));
-        SCF_SOLVER(cusolverDnSetStream(s->sol, s->st));
-        SCF_SOLVER(cusolverDnDsyevd_bufferSize(s->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb, s->Cob,
-                                               nb, s->W, &s->lwork));
-        SCF_CUDA(cudaMalloc((void**)&s->work, (size_t)std::max(1, s->lwork) * sizeof(double)));
-        s->bytes = (13 + 2 * NDIIS) * bytes + nb * sizeof(double) + ws + (size_t)s->lwork * sizeof(double) +
-                   sizeof(CycleScalars) + sizeof(int) + (4 + 2 * (size_t)nb) * sizeof(double);
+    SCF_RC(acquire_linalg(s));
+    SCF_SOLVER(cusolverDnDsyevd_bufferSize(s->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb, nullptr, nb,
+                                           nullptr, &s->lwork));
+    // every buffer of the job in one stream-ordered allocation (256-byte aligned pieces)
+    const size_t ws = 4u << 20;  // cuBLAS gets its workspace here, so it never allocates later
+    size_t off = 0;
+    auto take = [&](size_t b) {
+        const size_t o = off;
+        off += (b + 255) / 256 * 256;
+        return o;
+    };
+    double** mats[] = {&s->S, &s->H, &s->X, &s->P, &s->Pold, &s->F, &s->Fprev, &s->dP, &s->dF, &s->T1, &s->T2,
+                       &s->Fob, &s->Cob};
+    size_t o_mats[13], o_r[NDIIS], o_fo[NDIIS];
+    for (int k = 0; k < 13; ++k) o_mats[k] = take(bytes);
+    for (int k = 0; k < NDIIS; ++k) {
+        o_r[k] = take(bytes);
+        o_fo[k] = take(bytes);
     }
+    const size_t o_w = take(nb * sizeof(double)), o_info = take(sizeof(int)), o_sc = take(sizeof(CycleScalars));
+    const size_t o_aux = take((4 + 2 * (size_t)nb) * sizeof(double)), o_ws = take(ws);
+    const size_t o_work = take((size_t)std::max(1, s->lwork) * sizeof(double));
+    SCF_CUDA(cudaMallocAsync(&s->arena, off, s->st));
+    char* base = (char*)s->arena;
+    for (int k = 0; k < 13; ++k) *mats[k] = (double*)(base + o_mats[k]);
+    for (int k = 0; k < NDIIS; ++k) {
+        s->R[k] = (double*)(base + o_r[k]);
+        s->FO[k] = (double*)(base + o_fo[k]);
+    }
+    s->W = (double*)(base + o_w);
+    s->info = (int*)(base + o_info);
+    s->sc = (CycleScalars*)(base + o_sc);
+    s->aux = (double*)(base + o_aux);
+    s->blas_ws = base + o_ws;
+    s->work = (double*)(base + o_work);
+    s->bytes = off;
+    SCF_BLAS(cublasSetWorkspace(s->blas, s->blas_ws, ws));
     SCF_CUDA(cudaMemcpyAsync(s->S, S, bytes, cudaMemcpyHostToDevice, s->st));
     SCF_CUDA(cudaMemcpyAsync(s->H, hcore, bytes, cudaMemcpyHostToDevice, s->st));
     // residual history starts at 1000 everywhere, as the reference's resido

@@ -303,9 +303,10 @@ class DeviceSCFJob:
         Hc = np.ascontiguousarray(hcore, dtype=np.float64)
         Pc = None if p_guess is None else np.ascontiguousarray(p_guess, dtype=np.float64)
         out = ctypes.c_void_p()
-        with DEVICE_LOCK:
-            _check(_lib.hfgpu_scf_create(builder.h, int(nocc), float(enuc), _dp(Sc), _dp(Hc),
-                                         _dp(Pc) if Pc is not None else None, ctypes.byref(out)), "scf_create")
+        # the job's buffers come from the stream-ordered allocator on the
+        # builder's stream, so no library-wide lock is needed here
+        _check(_lib.hfgpu_scf_create(builder.h, int(nocc), float(enuc), _dp(Sc), _dp(Hc),
+                                     _dp(Pc) if Pc is not None else None, ctypes.byref(out)), "scf_create")
         self.s = out
 
     def run(self, maxiter: int = 25, conv: float = 1e-5, conve: float = 5e-8, fp32_cutoff: float = 0.0,
@@ -331,8 +332,7 @@ class DeviceSCFJob:
 
     def close(self):
         if getattr(self, "s", None):
-            with DEVICE_LOCK:
-                _lib.hfgpu_scf_destroy(self.s)
+            _lib.hfgpu_scf_destroy(self.s)
             self.s = None
 
     def __del__(self):

@@ -30,11 +30,7 @@ def one_electron(mol: Molecule, sh: ShellSet, gpu: bool = False):
     x = np.ascontiguousarray(mol.coords, dtype=np.float64)
     args = (ctypes.addressof(desc.struct), mol.natom, z.ctypes.data_as(d), x.ctypes.data_as(d),
             S.ctypes.data_as(d), T.ctypes.data_as(d), V.ctypes.data_as(d))
-    if gpu:
-        with fock.DEVICE_LOCK:  # it allocates: not while another thread records a graph
-            rc = fn(*args)
-    else:
-        rc = fn(*args)
+    rc = fn(*args)  # the GPU form allocates stream-ordered on its own stream: no lock needed
     if rc != 0:
         msg = lib.hfgpu_last_error().decode(errors="replace") if gpu else ""
         raise fock.HfgpuError(f"{fn.__name__} failed ({rc}) {msg}")
