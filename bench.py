@@ -338,6 +338,64 @@ def mixed_c20h42(fock, gold, dev):
             "abs_dE_fp64_vs_oracle": abs(r64.energy - gold["energy"])}
 
 
+def batch_study(fock, dev, reps: int = 5):
+    """Batching form on eight served-size molecules (C4H10 ... (H2O)12,
+    6-31G(d), atomic-density guess): the wall time of one full build of each,
+    (a) one after another through the device entry point (each build enqueues
+    its ~100-300 kernels and reads its survivor counts back once), (b) as
+    eight CUDA-graph replays, and (c) as one graph launch holding all eight
+    instances (hfgpu_batch_launch), with the kernels each launch runs."""
+    import torch
+    from hfcode_b200 import basis, molecules
+    bas = basis.load_basis("6-31G(d)")
+    mols = [molecules.alkane(4), molecules.alkane(8), molecules.alkane(12), molecules.alkane(16)] + \
+        [molecules.water_cluster(k, np.random.default_rng(k)) for k in (3, 6, 9, 12)]
+    fbs, Fs, Ps = [], [], []
+    for m in mols:
+        sh = basis.spread_basis(m, bas)
+        p = basis.density_superposition(m, bas, sh.nb)
+        fb = fock.FockBuilder(sh)
+        fb.fock_build_initial_diag(np.zeros((sh.nb, sh.nb)), p, THR)
+        fbs.append(fb)
+        Ps.append(torch.from_numpy(np.ascontiguousarray(p)).to(dev))
+        Fs.append(torch.zeros((sh.nb, sh.nb), dtype=torch.float64, device=dev))
+
+    def wall(fn):
+        ts = []
+        for _ in range(reps + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        return 1e3 * float(np.median(ts[1:]))
+
+    def eager():
+        for fb, F, P in zip(fbs, Fs, Ps):
+            fb.fock_build_device(F.data_ptr(), P.data_ptr(), THR, THR, 0.0)
+
+    l0 = sum(fb.launch_count() for fb in fbs)
+    t_eager = wall(eager)
+    k_eager = (sum(fb.launch_count() for fb in fbs) - l0) / (reps + 1)
+    for fb, F, P in zip(fbs, Fs, Ps):
+        fb.graph_capture(F.data_ptr(), P.data_ptr(), THR, THR, 0.0)
+
+    def replays():
+        for fb in fbs:
+            fb.graph_launch()
+
+    t_graph = wall(replays)
+    batch = fock.Batch(fbs)
+    t_batch = wall(lambda: batch.launch(0))
+    batch.close()
+    for fb in fbs:
+        fb.close()
+    return {"molecules": ["C4H10", "C8H18", "C12H26", "C16H34", "(H2O)3", "(H2O)6", "(H2O)9", "(H2O)12"],
+            "eager_ms": t_eager, "graph_replays_ms": t_graph, "one_batch_launch_ms": t_batch,
+            "kernels_per_round": k_eager, "host_launch_calls": {"eager": k_eager, "graph_replays": len(fbs),
+                                                                 "one_batch_launch": 1}}
+
+
 def served_study(n_jobs: int, rate: float, slots: int, n_plain: int):
     """The serving form: a seeded Poisson stream of RHF/6-31G(d) jobs
     (CnH2n+2 n <= 16, (H2O)k k <= 20; mixed precision at cutoff 1e-7) served
@@ -473,8 +531,8 @@ def main():
     achieved = cls_flops[top] / (st["ms"][top] * 1e-3) / 1e12
     peak_tf = fp64_peak / 1e3
     # DRAM bytes per LL|DL quartet (role kernels + scatter) from one ncu
-    # capture of the same kernels on C30H62 (271,664 LL|DL quartets per build;
-    # profiles/staged_class_kernels_c30h62.md), scaled by this build's count
+    # capture of these same kernels on n-C30H62 (271,664 LL|DL quartets per
+    # build), scaled by this build's LL|DL quartet count
     traffic = None
     if fock.CLASS_NAMES[top] == "LL|DL":
         traffic = LLDL_DRAM_BYTES_PER_QUARTET * float(st["pass"][top])
@@ -493,7 +551,10 @@ def main():
                     "peak_source": hbm_src}
     roof = {"bound": "fp64", "kernel": f"class {fock.CLASS_NAMES[top]} (role kernels + k_scatter_staged)",
             "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf,
-            "traffic": traffic, "traffic_unit": "bytes per build of the class", "hbm_view": hbm_view,
+            "traffic": traffic, "traffic_unit": "bytes per build of the class",
+            "traffic_source": "scaled: 2805 DRAM bytes per LL|DL quartet (role kernels + scatter) measured by ncu on "
+                              "n-C30H62 with these kernels, times this build's LL|DL quartet count",
+            "hbm_view": hbm_view,
             "peak_source": "measured FP64 FMA-chain probe on this device (MEASURED_PEAKS.json has no FP64 figure)",
             "all_classes_tflops": float(cls_flops.sum() / (st["ms"].sum() * 1e-3) / 1e12),
             "class_ms": {fock.CLASS_NAMES[c]: round(float(st["ms"][c]), 3) for c in range(fock.NCLASS) if st["ms"][c] > 0},
@@ -513,6 +574,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_mixed:
         out["mixed"] = mixed_study(fock, mol, sh, [float(x) for x in args.mixed_cutoffs.split(",")], dev)
     if rank == 0 and world == 1 and not args.no_serve:
+        out["batching"] = batch_study(fock, dev)
         out["served"] = served_study(args.serve_jobs, args.serve_rate, 8, args.serve_plain)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_oracle_builds(sh, p, 1, 2, args.cpu_stride, calibrate=True)

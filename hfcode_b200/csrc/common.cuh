@@ -395,12 +395,26 @@ __device__ __forceinline__ void scatter_async(const E* __restrict__ e, size_t st
     const double* __restrict__ Bbd = Pb + __ldg(boff + bra.sb * nsh + ket.sb);
     const double* __restrict__ Bcd = Pb + __ldg(boff + ket.sa * nsh + ket.sb);
     auto Ga = [&](int r, int c) { return G + r + (size_t)c * nb; };
-    // consecutive quartets mostly share their bra pair: when the whole warp
-    // does, its J_ab sums (same addresses) are reduced across the warp and
-    // added once
-    const unsigned long long bkey = ((unsigned long long)bra.aoa << 32) | (unsigned)bra.aob;
-    const bool wuni = __all_sync(0xffffffffu, bkey == __shfl_sync(0xffffffffu, bkey, 0));
+    // The quartets of a warp are consecutive entries of a compacted list:
+    // they mostly share their bra pair, and the active lists are ordered by
+    // first shell within each primitive-count group, so they mostly share the
+    // ket's first shell too.  A block element whose row and column shells are
+    // the same in every lane has one address for the whole warp: its sums are
+    // reduced across the warp and added with one atomic.
     const int lane = threadIdx.x & 31;
+    auto same = [](int x) { return __all_sync(0xffffffffu, x == __shfl_sync(0xffffffffu, x, 0)); };
+    const bool ua = same(a0), ub = same(b0), uc = same(c0), ud = same(d0);
+    const bool wuni = ua && ub;
+    // every lane calls this with the same `uni` (lanes without a quartet add 0)
+    auto emit = [&](double* addr, double v, bool uni) {
+        if (uni) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) atomicAdd(addr, v);
+        } else if (act) {
+            atomicAdd(addr, v);
+        }
+    };
     E* eb = sm + tid;                      // [NBUF][SLAB][T], this thread's column
     E* pk = sm + NBUF * SLAB * T + tid;    // [NB*NC] P_bc then [NB*ND] P_bd
     auto issue = [&](int slab) {
@@ -473,38 +487,31 @@ __device__ __forceinline__ void scatter_async(const E* __restrict__ e, size_t st
             }
         }
 #pragma unroll
-        for (int j = 0; j < NB; ++j) {
-            double v = act ? (double)(s2 * jab[j]) : 0.0;
-            if (wuni) {
+        for (int j = 0; j < NB; ++j) emit(Ga(a0 + i, b0 + j), act ? (double)(s2 * jab[j]) : 0.0, wuni);
+        if (!jonly) {
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                if (lane == 0) atomicAdd(Ga(a0 + i, b0 + j), v);
-            } else if (act) {
-                atomicAdd(Ga(a0 + i, b0 + j), v);
-            }
-        }
-        if (!jonly && act) {
+            for (int k = 0; k < NC; ++k) emit(Ga(a0 + i, c0 + k), act ? (double)(hs * kac[k]) : 0.0, ua && uc);
 #pragma unroll
-            for (int k = 0; k < NC; ++k) atomicAdd(Ga(a0 + i, c0 + k), (double)(hs * kac[k]));
-#pragma unroll
-            for (int l = 0; l < ND; ++l) atomicAdd(Ga(a0 + i, d0 + l), (double)(hs * kad[l]));
+            for (int l = 0; l < ND; ++l) emit(Ga(a0 + i, d0 + l), act ? (double)(hs * kad[l]) : 0.0, ua && ud);
         }
     }
     cp_async_wait<0>();
-    if (!act) return;
 #pragma unroll
     for (int k = 0; k < NC; ++k)
 #pragma unroll
-        for (int l = 0; l < ND; ++l) atomicAdd(Ga(c0 + k, d0 + l), (double)(s2 * jcd[k * ND + l]));
+        for (int l = 0; l < ND; ++l)
+            emit(Ga(c0 + k, d0 + l), act ? (double)(s2 * jcd[k * ND + l]) : 0.0, uc && ud);
     if (jonly) return;
 #pragma unroll
     for (int j = 0; j < NB; ++j)
 #pragma unroll
-        for (int k = 0; k < NC; ++k) atomicAdd(Ga(b0 + j, c0 + k), (double)(hs * kbc[j * NC + k]));
+        for (int k = 0; k < NC; ++k)
+            emit(Ga(b0 + j, c0 + k), act ? (double)(hs * kbc[j * NC + k]) : 0.0, ub && uc);
 #pragma unroll
     for (int j = 0; j < NB; ++j)
 #pragma unroll
-        for (int l = 0; l < ND; ++l) atomicAdd(Ga(b0 + j, d0 + l), (double)(hs * kbd[j * ND + l]));
+        for (int l = 0; l < ND; ++l)
+            emit(Ga(b0 + j, d0 + l), act ? (double)(hs * kbd[j * ND + l]) : 0.0, ub && ud);
 }
 
 // Post-screen (max |e| over all roles < thr, fock_build_non_diag.f90:69) and

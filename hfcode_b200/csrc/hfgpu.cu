@@ -582,11 +582,16 @@ int build_active(hfgpu_handle* h) {
             }
         }
         h->last_ref[GPU_TO_REF[t]] = last;
-        // active set, re-ordered for the GPU: primitive count, then Schwarz
+        // active set, re-ordered for the GPU: primitive count, first shell, then Schwarz
         std::vector<int> act(ord.begin(), ord.begin() + last);
         std::stable_sort(act.begin(), act.end(), [&](int x, int y) {
             int nx = h->pairs[t][x].g.np, ny = h->pairs[t][y].g.np;
             if (nx != ny) return nx > ny;
+            // within a primitive-count group by first shell, so the 32
+            // quartets of a warp mostly share it (the staged scatter then
+            // adds their K blocks with one atomic per element)
+            const int sx = h->pairs[t][x].g.sa, sy = h->pairs[t][y].g.sa;
+            if (sx != sy) return sx < sy;
             return h->schw[t][x] > h->schw[t][y];
         });
         std::vector<GPair> ap(last);

@@ -142,24 +142,24 @@ inline void build_boys_table(std::vector<double>& bt, std::vector<float>& btf) {
 // Structure-of-arrays copy of primitive pairs: 8 arrays of n doubles
 // (p, Px, Py, Pz, K, w1, w2, 1/(2p)) back to back.
 inline std::vector<double> prims_soa(const std::vector<GPrim>& prims) {
+    // four arrays of (field, field) pairs, 2n doubles each (see PrimSoA)
     const size_t n = prims.size();
     std::vector<double> s(8 * n);
     for (size_t i = 0; i < n; ++i) {
-        s[i] = prims[i].p;
-        s[n + i] = prims[i].P[0];
-        s[2 * n + i] = prims[i].P[1];
-        s[3 * n + i] = prims[i].P[2];
-        s[4 * n + i] = prims[i].K;
-        s[5 * n + i] = prims[i].w1;
-        s[6 * n + i] = prims[i].w2;
-        s[7 * n + i] = 0.5 / prims[i].p;
+        s[2 * i] = prims[i].p;
+        s[2 * i + 1] = prims[i].P[0];
+        s[2 * n + 2 * i] = prims[i].P[1];
+        s[2 * n + 2 * i + 1] = prims[i].P[2];
+        s[4 * n + 2 * i] = prims[i].K;
+        s[4 * n + 2 * i + 1] = prims[i].w1;
+        s[6 * n + 2 * i] = prims[i].w2;
+        s[6 * n + 2 * i + 1] = 0.5 / prims[i].p;
     }
     return s;
 }
-
 inline PrimSoA soa_view(const double* base, size_t n) {
-    return PrimSoA{base, base + n, base + 2 * n, base + 3 * n, base + 4 * n, base + 5 * n, base + 6 * n,
-                   base + 7 * n};
+    const PrimVec* v = reinterpret_cast<const PrimVec*>(base);
+    return PrimSoA{v, v + n, v + 2 * n, v + 3 * n};
 }
 
 }  // namespace hfgpu

@@ -191,6 +191,9 @@ struct hfgpu_scf {
     bool diis = false, fullfock = true, converged = false;
     int nusediis = 0, nfull = 0, nfullb = 0, ndelta = 0;
     double thresh = 0.0, deltae = 0.0, deltap = 0.0;
+    int sp2_steps = 0;
+    double ms_build = 0.0, ms_density = 0.0;
+    cudaEvent_t ev[4] = {};      // build start/end, density start/end of the current cycle
     int slot[NDIIS] = {};        // history position -> buffer (position 0: newest)
     double eo[NDIIS] = {};       // energies of the history positions
     double B[NDIIS][NDIIS] = {}; // <R_j, R_k> by history position
@@ -277,13 +280,18 @@ int density_by_purification(hfgpu_scf* s, const double* Fo, double* P) {
     k_gershgorin_bounds<<<1, 1024, 0, s->st>>>(s->aux + 4, s->aux + 4 + nb, nb, bounds);
     k_sp2_start<<<blocks, 256, 0, s->st>>>(Fo, bounds, X, nb);
     SCF_CUDA(cudaGetLastError());
-    constexpr int BLOCK = 8, MAXSTEP = 160;
-    for (int step = 0; step < MAXSTEP; step += BLOCK) {
-        for (int k = 0; k < BLOCK; ++k) {
+    // the first check after 16 steps (the start needs ~log2 of the spectral
+    // range over the gap of them), then every 4
+    constexpr int FIRST = 16, BLOCK = 4, MAXSTEP = 160;
+    for (int step = 0; step < MAXSTEP;) {
+        const int nstep = step == 0 ? FIRST : BLOCK;
+        for (int k = 0; k < nstep; ++k) {
             SCF_RC(gemm(s, false, false, 1.0, X, X, 0.0, X2));
             k_traces<<<1, 256, 0, s->st>>>(X, X2, nb, tr);
             k_sp2_step<<<blocks, 256, 0, s->st>>>(X, X2, tr, (double)s->nocc, n2);
         }
+        step += nstep;
+        s->sp2_steps += nstep;
         SCF_CUDA(cudaGetLastError());
         double h_tr[2];
         SCF_CUDA(cudaMemcpyAsync(h_tr, tr, sizeof(h_tr), cudaMemcpyDeviceToHost, s->st));
@@ -355,6 +363,8 @@ int acquire_linalg(hfgpu_scf* s) {
 
 void release(hfgpu_scf* s) {
     if (s->st) cudaStreamSynchronize(s->st);
+    for (auto& e : s->ev)
+        if (e) cudaEventDestroy(e);
     if (s->arena) cudaFreeAsync(s->arena, s->st);
     if (s->st) cudaStreamSynchronize(s->st);
     if (s->blas && s->sol) {
@@ -379,6 +389,7 @@ int create(hfgpu_handle* h, int nocc, double enuc, const double* S, const double
     s->st = (cudaStream_t)hfgpu_stream(h);
     const size_t n2 = (size_t)nb * nb, bytes = n2 * sizeof(double);
     SCF_RC(acquire_linalg(s));
+    for (auto& e : s->ev) SCF_CUDA(cudaEventCreate(&e));
     SCF_SOLVER(cusolverDnDsyevd_bufferSize(s->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb, nullptr, nb,
                                            nullptr, &s->lwork));
     // every buffer of the job in one stream-ordered allocation (256-byte aligned pieces)
@@ -478,6 +489,7 @@ int run(hfgpu_scf* s, const hfgpu_scf_params& prm, hfgpu_scf_result* res) {
     while (!converged && s->it < prm.maxiter) {
         const int it = ++s->it;
         const double eeold = eelec;
+        SCF_CUDA(cudaEventRecord(s->ev[0], s->st));
         SCF_RC(copy(s, s->F, s->H));
         if (fullfock && it == 1) {  // direct_hartreefock.f90:101-105 (fullfock stays set)
             SCF_RC(hfgpu_fock_build_initial_diag_device(h, s->F, s->P, thresh));
@@ -500,6 +512,7 @@ int run(hfgpu_scf* s, const hfgpu_scf_params& prm, hfgpu_scf_result* res) {
             if (++nfull == 15) fullfock = true;
             ++ndelta;
         }
+        SCF_CUDA(cudaEventRecord(s->ev[1], s->st));
         SCF_RC(copy(s, s->Fprev, s->F));
         // fob = X F X^T; residual X^T (F P S - S P F) X, with S P F = (F P S)^T
         SCF_RC(gemm(s, false, false, 1.0, s->X, s->F, 0.0, s->T1));
@@ -601,8 +614,16 @@ int run(hfgpu_scf* s, const hfgpu_scf_params& prm, hfgpu_scf_result* res) {
             break;
         }
         SCF_RC(copy(s, s->Pold, s->P));
+        SCF_CUDA(cudaEventRecord(s->ev[2], s->st));
         if (vectors) SCF_RC(density_from_cob(s, s->P));
         else SCF_RC(density_by_purification(s, s->Fob, s->P));
+        SCF_CUDA(cudaEventRecord(s->ev[3], s->st));
+        SCF_CUDA(cudaEventSynchronize(s->ev[3]));
+        float mb = 0.f, md = 0.f;
+        cudaEventElapsedTime(&mb, s->ev[0], s->ev[1]);
+        cudaEventElapsedTime(&md, s->ev[2], s->ev[3]);
+        s->ms_build += mb;
+        s->ms_density += md;
     }
     SCF_CUDA(cudaStreamSynchronize(s->st));
     if (res) {
@@ -614,6 +635,9 @@ int run(hfgpu_scf* s, const hfgpu_scf_params& prm, hfgpu_scf_result* res) {
         res->converged = converged ? 1 : 0;
         res->full_builds = nfullb;
         res->delta_builds = ndelta;
+        res->sp2_steps = s->sp2_steps;
+        res->ms_build = s->ms_build;
+        res->ms_density = s->ms_density;
     }
     return HFGPU_OK;
 }

@@ -43,28 +43,46 @@ struct GPair {
     int ps, pad;   // primitive stride
 };
 
-// Primitive pairs as structure of arrays (fields of GPrim).
+// Primitive pairs as four arrays of 16-byte pairs of fields of GPrim:
+// (p, Px), (Py, Pz), (K, w1), (w2, 1/(2p)); one primitive pair is four
+// vector loads instead of eight scalar ones.
+struct alignas(16) PrimVec {
+    double a, b;
+};
 struct PrimSoA {
-    const double* p;
-    const double* x;
-    const double* y;
-    const double* z;
-    const double* K;
-    const double* w1;
-    const double* w2;
-    const double* h;   // 1/(2p), precomputed on the host
+    const PrimVec* v0;  // p, Px
+    const PrimVec* v1;  // Py, Pz
+    const PrimVec* v2;  // K, w1
+    const PrimVec* v3;  // w2, 1/(2p)
 };
 
 __device__ __forceinline__ GPrim load_prim(const PrimSoA& s, int i) {
+#ifdef __CUDA_ARCH__
+    const double2 a = __ldg(reinterpret_cast<const double2*>(s.v0) + i);
+    const double2 b = __ldg(reinterpret_cast<const double2*>(s.v1) + i);
+    const double2 c = __ldg(reinterpret_cast<const double2*>(s.v2) + i);
+    const double2 d = __ldg(reinterpret_cast<const double2*>(s.v3) + i);
     GPrim g;
-    g.p = __ldg(s.p + i);
-    g.P[0] = __ldg(s.x + i);
-    g.P[1] = __ldg(s.y + i);
-    g.P[2] = __ldg(s.z + i);
-    g.K = __ldg(s.K + i);
-    g.w1 = __ldg(s.w1 + i);
-    g.w2 = __ldg(s.w2 + i);
-    g.pad = __ldg(s.h + i);  // 1/(2p)
+    g.p = a.x;
+    g.P[0] = a.y;
+    g.P[1] = b.x;
+    g.P[2] = b.y;
+    g.K = c.x;
+    g.w1 = c.y;
+    g.w2 = d.x;
+    g.pad = d.y;  // 1/(2p)
+#else
+    const PrimVec a = s.v0[i], b = s.v1[i], c = s.v2[i], d = s.v3[i];
+    GPrim g;
+    g.p = a.a;
+    g.P[0] = a.b;
+    g.P[1] = b.a;
+    g.P[2] = b.b;
+    g.K = c.a;
+    g.w1 = c.b;
+    g.w2 = d.a;
+    g.pad = d.b;
+#endif
     return g;
 }
 

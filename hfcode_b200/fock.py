@@ -61,7 +61,8 @@ class ScfResult(ctypes.Structure):
     """hfgpu_scf_result (include/hfgpu_scf.h)."""
     _fields_ = [("energy", ctypes.c_double), ("eelec", ctypes.c_double), ("deltae", ctypes.c_double),
                 ("deltap", ctypes.c_double), ("cycles", ctypes.c_int), ("converged", ctypes.c_int),
-                ("full_builds", ctypes.c_int), ("delta_builds", ctypes.c_int)]
+                ("full_builds", ctypes.c_int), ("delta_builds", ctypes.c_int), ("sp2_steps", ctypes.c_int),
+                ("ms_build", ctypes.c_double), ("ms_density", ctypes.c_double)]
 
 
 def _load():
