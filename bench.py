@@ -222,6 +222,11 @@ def mixed_study(fock, mol, sh, cutoffs, dev):
     scf.device_hartreefock(wmol, wsh, fbw, p_guess=basis.density_superposition(wmol, bas, wsh.nb), conve=1e-9,
                            conv=1e-6, maxiter=80, fp32_cutoff=1e-5)
     fbw.close()
+    # and one untimed SCF of this molecule: the stream-ordered memory pool
+    # grows to this job's size once, instead of inside the first timed run
+    fbw = fock.FockBuilder(sh)
+    scf.device_hartreefock(mol, sh, fbw, p_guess=p0, conve=1e-9, conv=1e-6, maxiter=80, ints=ints)
+    fbw.close()
     for rep in range(3):
         for label, cut in (("device_scf_fp64", 0.0), ("device_scf_mixed_1e-05", 1e-5)):
             fbd = fock.FockBuilder(sh)
