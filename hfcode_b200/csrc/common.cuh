@@ -598,6 +598,9 @@ struct ClassKernels {
     int scat_smem;                // dynamic shared memory of scat (bytes)
     StagedKernel scat32;          // scatter of FP32 chunks (float rows), or nullptr
     int scat32_smem;
+    // every role of a stage in one launch (gridDim.y = roles), for small chunks
+    StagedKernel ma64, ma32;      // stage-A roles (staged3)
+    StagedKernel mb64, mb32;      // output / HRR roles
     int bi, ki, L, nout;
 };
 

@@ -629,6 +629,21 @@ def acc_groups(g: "ClassGen", group: int = ACC_GROUP):
     return best[1]
 
 
+def merged_kernel(kname: str, bodies: List[str], minb: int = 2) -> str:
+    """All roles of one stage in one launch: block row blockIdx.y runs role
+    blockIdx.y (every thread of a block runs the same role).  Used for small
+    chunks, where one launch per role would leave most SMs idle and the
+    launches themselves would set the time."""
+    cases = "\n".join(f"        case {r}: {b}_body(a); break;" for r, b in enumerate(bodies))
+    return f"""
+__global__ void __launch_bounds__(ND_THREADS, {minb}) {kname}(StagedArgs a) {{
+    switch (blockIdx.y) {{
+{cases}
+        default: break;
+    }}
+}}"""
+
+
 def class_source(ci: int, bi: int, ki: int):
     """Header (device functions) and translation unit (kernels) of one
     quartet class; returns (cuh_text, cu_text, info).
@@ -679,7 +694,7 @@ def class_source(ci: int, bi: int, ki: int):
                                f"mx = fmax(mx, fabs(v)); }}" for i, n in enumerate(outs))
             tab = "a.boysf" if f32 else "a.boys"
             return f"""
-__global__ void __launch_bounds__(ND_THREADS, 2) {kname}(StagedArgs a) {{
+__device__ __forceinline__ void {kname}_body(const StagedArgs& a) {{
     // Boys table of order L read through the L1 cache: with a few primitive
     // quartets per shell quartet, staging it in shared memory per block
     // costs more than the lookups it serves
@@ -695,7 +710,8 @@ __global__ void __launch_bounds__(ND_THREADS, 2) {kname}(StagedArgs a) {{
     {real}* out = reinterpret_cast<{real}*>(a.out);  // FP32 chunks keep FP32 rows
 {stores}
     a.mx[(size_t){r} * a.stride + t] = mx;
-}}"""
+}}
+__global__ void __launch_bounds__(ND_THREADS, 2) {kname}(StagedArgs a) {{ {kname}_body(a); }}"""
 
         for r, outs in enumerate(roles):
             code, _ = g.emit_role(f"{g.name}_r{r}", outs)
@@ -705,6 +721,9 @@ __global__ void __launch_bounds__(ND_THREADS, 2) {kname}(StagedArgs a) {{
             code32, _ = g32.emit_role(f"{g32.name}_r{r}", outs)
             funcs.append(code32)
             kern.append(s2_kernel(f"k_s2f_{g.tag}_r{r}", f"eri_{g.tag}_f32_r{r}", outs, r, True))
+        kern.append(merged_kernel(f"k_s2m_{g.tag}", [f"k_s2_{g.tag}_r{r}" for r in range(len(roles))]))
+        kern.append(merged_kernel(f"k_s2mf_{g.tag}", [f"k_s2f_{g.tag}_r{r}" for r in range(len(roles32))]))
+        reg.append(f"    k->mb64 = k_s2m_{g.tag};\n    k->mb32 = k_s2mf_{g.tag};")
         reg.append(f"    k->mode = 1;\n    k->nacc = 0;\n    k->nrole_a = 0;\n    k->nrole_b = {len(roles)};\n"
                    f"    k->nrole_b32 = {len(roles32)};")
         for r in range(len(roles)):
@@ -740,7 +759,7 @@ __global__ void __launch_bounds__(ND_THREADS, 2) {kname}(StagedArgs a) {{
                 code, _ = gen.emit_acc_role(fname, gr)
                 funcs.append(code)
                 kern.append(f"""
-__global__ void __launch_bounds__(ND_THREADS, 2) {kpre}_{g.tag}_r{r}(StagedArgs a) {{
+__device__ __forceinline__ void {kpre}_{g.tag}_r{r}_body(const StagedArgs& a) {{
     const {real}* __restrict__ sboys = {tab} + (size_t){g.L} * BOYS_BLK;  // Boys table of order L, through L1
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= staged_count(a)) return;
@@ -748,7 +767,8 @@ __global__ void __launch_bounds__(ND_THREADS, 2) {kpre}_{g.tag}_r{r}(StagedArgs 
     const GPair bra = a.bra[q.x];
     const GPair ket = a.ket[q.y];
     {fname}(bra, ket, a.prims, sboys, reinterpret_cast<{real}*>(a.acc) + (size_t){base} * a.stride + t, a.stride);
-}}""")
+}}
+__global__ void __launch_bounds__(ND_THREADS, 2) {kpre}_{g.tag}_r{r}(StagedArgs a) {{ {kpre}_{g.tag}_r{r}_body(a); }}""")
                 base += len(gr)
         og = prm["out_group3"]
         outroles = [list(range(i, min(i + og, g.nout))) for i in range(0, g.nout, og)]
@@ -759,7 +779,7 @@ __global__ void __launch_bounds__(ND_THREADS, 2) {kpre}_{g.tag}_r{r}(StagedArgs 
             for kname, fname, real in ((f"k_sb_{g.tag}_r{r}", f"hrr_{g.tag}_r{r}", "double"),
                                        (f"k_sbf_{g.tag}_r{r}", f"hrr_{g.tag}_f32_r{r}", "float")):
                 kern.append(f"""
-__global__ void __launch_bounds__(ND_THREADS) {kname}(StagedArgs a) {{
+__device__ __forceinline__ void {kname}_body(const StagedArgs& a) {{
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= staged_count(a)) return;
     const uint2 q = staged_quartet(a, t);
@@ -768,7 +788,14 @@ __global__ void __launch_bounds__(ND_THREADS) {kname}(StagedArgs a) {{
     a.mx[(size_t){r} * a.stride + t] =
         {fname}(bra, ket, reinterpret_cast<const {real}*>(a.acc) + t,
                 reinterpret_cast<{real}*>(a.out) + (size_t){outs[0]} * a.stride + t, a.stride);
-}}""")
+}}
+__global__ void __launch_bounds__(ND_THREADS) {kname}(StagedArgs a) {{ {kname}_body(a); }}""")
+        kern.append(merged_kernel(f"k_sam_{g.tag}", [f"k_sa_{g.tag}_r{r}" for r in range(len(groups))]))
+        kern.append(merged_kernel(f"k_samf_{g.tag}", [f"k_saf_{g.tag}_r{r}" for r in range(len(groups32))]))
+        kern.append(merged_kernel(f"k_sbm_{g.tag}", [f"k_sb_{g.tag}_r{r}" for r in range(len(outroles))], minb=1))
+        kern.append(merged_kernel(f"k_sbmf_{g.tag}", [f"k_sbf_{g.tag}_r{r}" for r in range(len(outroles))], minb=1))
+        reg.append(f"    k->ma64 = k_sam_{g.tag};\n    k->ma32 = k_samf_{g.tag};\n"
+                   f"    k->mb64 = k_sbm_{g.tag};\n    k->mb32 = k_sbmf_{g.tag};")
         reg.append(f"    k->mode = 2;\n    k->nacc = {len(keyidx)};\n    k->nrole_a = {len(groups)};\n"
                    f"    k->nrole_a32 = {len(groups32)};\n"
                    f"    k->nrole_b = {len(outroles)};\n    k->nrole_b32 = {len(outroles)};")

@@ -462,6 +462,16 @@ int launch_symm(hfgpu_handle* h, double* F, const double* G = nullptr) {
     return HFGPU_OK;
 }
 
+// Whether a chunk runs every role of a stage in one launch (gridDim.y =
+// roles): when one launch per role would fill less than the GPU's SMs twice
+// over.  Large chunks keep one launch per role, so that every warp on an SM
+// runs the same role's code (these FP64 recursions are long straight-line
+// programs, and an SM running several of them thrashes its instruction
+// cache); small chunks gain more from filling the SMs and launching less.
+bool merge_roles(const hfgpu_handle* h, const ClassKernels& K, int blocks, int roles) {
+    return K.mb64 && roles > 1 && (long long)blocks * roles <= 2LL * h->nsm;
+}
+
 // Diagonal builder of a staged pair type: chunks of its pairs through the
 // class's roles and k_scatter_diag.
 int run_staged_diag(hfgpu_handle* h, int t, int mode, const double* P, double thr, double* G, const double* md) {
@@ -494,15 +504,26 @@ int run_staged_diag(hfgpu_handle* h, int t, int mode, const double* P, double th
         a.md = md;
         a.nsh = h->nsh;
         const int blocks = (m + ND_THREADS - 1) / ND_THREADS;
-        for (int r = 0; r < K.nrole_a; ++r) {
+        if (merge_roles(h, K, blocks, std::max(K.nrole_a, K.nrole_b))) {
+            if (K.nrole_a > 0) {
+                ++h->launches;
+                K.ma64<<<dim3(blocks, K.nrole_a), ND_THREADS, 0, h->stream>>>(a);
+                HF_CHECK(cudaGetLastError());
+            }
             ++h->launches;
-            K.sa64[r]<<<blocks, ND_THREADS, 0, h->stream>>>(a);
+            K.mb64<<<dim3(blocks, K.nrole_b), ND_THREADS, 0, h->stream>>>(a);
             HF_CHECK(cudaGetLastError());
-        }
-        for (int r = 0; r < K.nrole_b; ++r) {
-            ++h->launches;
-            K.sb64[r]<<<blocks, ND_THREADS, 0, h->stream>>>(a);
-            HF_CHECK(cudaGetLastError());
+        } else {
+            for (int r = 0; r < K.nrole_a; ++r) {
+                ++h->launches;
+                K.sa64[r]<<<blocks, ND_THREADS, 0, h->stream>>>(a);
+                HF_CHECK(cudaGetLastError());
+            }
+            for (int r = 0; r < K.nrole_b; ++r) {
+                ++h->launches;
+                K.sb64[r]<<<blocks, ND_THREADS, 0, h->stream>>>(a);
+                HF_CHECK(cudaGetLastError());
+            }
         }
         ++h->launches;
         (mode ? K.dscat1 : K.dscat0)<<<blocks, ND_THREADS, 0, h->stream>>>(a);
@@ -774,15 +795,28 @@ int run_staged(hfgpu_handle* h, int c, int prec, long long n, const double* P, d
         a.f32 = prec;
         a.stats = h->d_stats + c;
         const int blocks = (m + ND_THREADS - 1) / ND_THREADS;
-        for (int r = 0; r < (prec ? K.nrole_a32 : K.nrole_a); ++r) {
+        const int na = prec ? K.nrole_a32 : K.nrole_a;
+        if (merge_roles(h, K, blocks, std::max(na, a.nroles))) {
+            // a small chunk: every role of a stage in one launch, side by side
+            if (na > 0) {
+                ++h->launches;
+                (prec ? K.ma32 : K.ma64)<<<dim3(blocks, na), ND_THREADS, 0, stream>>>(a);
+                HF_CHECK(cudaGetLastError());
+            }
             ++h->launches;
-            (prec ? K.sa32[r] : K.sa64[r])<<<blocks, ND_THREADS, 0, stream>>>(a);
+            (prec ? K.mb32 : K.mb64)<<<dim3(blocks, a.nroles), ND_THREADS, 0, stream>>>(a);
             HF_CHECK(cudaGetLastError());
-        }
-        for (int r = 0; r < a.nroles; ++r) {
-            ++h->launches;
-            (prec ? K.sb32[r] : K.sb64[r])<<<blocks, ND_THREADS, 0, stream>>>(a);
-            HF_CHECK(cudaGetLastError());
+        } else {
+            for (int r = 0; r < na; ++r) {
+                ++h->launches;
+                (prec ? K.sa32[r] : K.sa64[r])<<<blocks, ND_THREADS, 0, stream>>>(a);
+                HF_CHECK(cudaGetLastError());
+            }
+            for (int r = 0; r < a.nroles; ++r) {
+                ++h->launches;
+                (prec ? K.sb32[r] : K.sb64[r])<<<blocks, ND_THREADS, 0, stream>>>(a);
+                HF_CHECK(cudaGetLastError());
+            }
         }
         ++h->launches;
         if (prec && K.scat32) K.scat32<<<blocks, ND_THREADS, K.scat32_smem, stream>>>(a);  // float rows
