@@ -176,3 +176,35 @@ def test_default_scratch_follows_the_molecule():
         out.append(f)
         fb.close()
     assert np.max(np.abs(out[0] - out[1])) < 1e-11
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["benzene", "alkane2_mix"])
+def test_merged_and_separate_role_launches_agree(name):
+    """Small chunks run every role of a stage in one launch (gridDim.y =
+    roles); HFGPU_MERGE_BLOCKS=0 at handle creation forces one launch per
+    role.  Both give the oracle's F and agree with each other to rounding."""
+    import os
+    from hfcode_b200.fock import FockBuilder
+    _, _, sh, p0 = system(name)
+    nb = sh.nb
+    p = perturbed_density(p0, 9)
+    out = {}
+    old = os.environ.get("HFGPU_MERGE_BLOCKS")
+    try:
+        for label, val in (("separate", "0"), ("merged", "1000000")):
+            os.environ["HFGPU_MERGE_BLOCKS"] = val
+            fb = FockBuilder(sh)
+            f = np.zeros((nb, nb))
+            fb.fock_build_initial_diag(f, p0, 1e-10)
+            fb.fock_build_non_diag(f, p, 1e-10)
+            fb.fock_build_non_diag_mixed(f, p, 1e-10, 1e-6)
+            out[label] = (f, fb.launch_count())
+            fb.close()
+    finally:
+        if old is None:
+            os.environ.pop("HFGPU_MERGE_BLOCKS", None)
+        else:
+            os.environ["HFGPU_MERGE_BLOCKS"] = old
+    assert np.max(np.abs(out["separate"][0] - out["merged"][0])) < 1e-11
+    assert out["merged"][1] < out["separate"][1]  # fewer launches
