@@ -56,6 +56,9 @@ typedef struct {
     int converged;
     int full_builds;    /* Fock builds with the full density */
     int delta_builds;   /* incremental (dP) builds */
+    int sp2_steps;      /* purification steps, all cycles */
+    double ms_build;    /* device time in the Fock builds, all cycles (CUDA events) */
+    double ms_density;  /* device time forming densities (purification or eigensolve) */
 } hfgpu_scf_result;
 
 void hfgpu_scf_defaults(hfgpu_scf_params* prm);
