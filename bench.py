@@ -410,6 +410,7 @@ def served_study(n_jobs: int, rate: float, slots: int, n_plain: int):
     from hfcode_b200 import serve
     jobs = serve.make_stream(n_jobs, rate)
     srv = serve.Server(64 << 30, slots, fp32_cutoff=1e-7)
+    srv.warmup()  # one tiny job per slot first (handles, memory pool), outside the stream
     served = srv.serve(jobs)
     plain_jobs = serve.make_stream(n_plain, 0.0)
     plain = serve.serve_sequential(plain_jobs, serve.Server(64 << 30, 1, fp32_cutoff=1e-7))
