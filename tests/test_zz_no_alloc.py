@@ -22,12 +22,15 @@ def test_static_scratch_diag_matches_fock_build_diag():
     import torch
 
     from hfcode_b200 import fock
+    from oracle import pyoracle
 
     _, _, sh, p0 = system("benzene")
     nb = sh.nb
     fb = fock.FockBuilder(sh)
     f0 = np.zeros((nb, nb))
     fb.fock_build_initial_diag(f0, p0, 1e-10)
+    orc = pyoracle.Oracle(sh)  # the CPU restatement of fock_build_diag, as a second check
+    orc.fock_build_initial_diag(np.zeros((nb, nb)), p0, 1e-10)
     dev = torch.device("cuda", torch.cuda.current_device())
     for call, seed in enumerate((5, 6)):  # two calls in a row share the scratch
         p = perturbed_density(p0, seed)
@@ -41,6 +44,9 @@ def test_static_scratch_diag_matches_fock_build_diag():
         torch.cuda.synchronize()
         got = F.cpu().numpy()
         assert np.max(np.abs(got - ref)) < TOL, (call, np.max(np.abs(got - ref)))
+        fo = np.full((nb, nb), 0.5)
+        orc.fock_build_diag(fo, p, 1e-10)
+        assert np.max(np.abs(got - fo)) < TOL, (call, np.max(np.abs(got - fo)))
     fb.close()
 
 
