@@ -69,6 +69,37 @@ namespace hfgpu {
 // error text for entry points in other translation units (onee.cu)
 void set_last_error(const std::string& msg) { g_err = msg; }
 std::recursive_mutex& device_mutex() { return g_dev_mu; }
+
+// The library's stream-ordered memory pool on the current device, created
+// on first use with no release threshold: memory a finished handle or job
+// frees stays in the pool for the next one instead of going back to the
+// driver at every synchronisation (which would map it again for the next
+// served job).  It is released when the process exits.
+cudaMemPool_t memory_pool() {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pools[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+        unsigned long long keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools[dev] = pool;
+    }
+    return pools[dev];
+}
+
+cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t st) {
+    cudaMemPool_t pool = memory_pool();
+    if (!pool) return cudaMallocAsync(p, bytes, st);
+    return cudaMallocFromPoolAsync(p, bytes, pool, st);
+}
 }  // namespace hfgpu
 
 namespace {
@@ -373,14 +404,15 @@ int set_err(int code, const std::string& msg) {
     return code;
 }
 
-// Device buffers of a handle come from the stream-ordered allocator on the
-// handle's stream: cudaFreeAsync, unlike cudaFree, does not synchronise the
-// whole device, so a served job that finishes does not stall the jobs still
-// running on the GPU.
+// Device buffers of a handle come from the library's stream-ordered pool on
+// the handle's stream: cudaFreeAsync, unlike cudaFree, does not synchronise
+// the whole device, so a served job that finishes does not stall the jobs
+// still running on the GPU.  These calls need no lock: a capture in another
+// thread (thread-local mode) is unaffected by them.
 template <typename T>
 int dalloc(T** p, size_t n, cudaStream_t st) {
     if (n == 0) n = 1;
-    cudaError_t e = cudaMallocAsync((void**)p, n * sizeof(T), st);
+    cudaError_t e = pool_alloc((void**)p, n * sizeof(T), st);
     if (e != cudaSuccess) {
         *p = nullptr;
         g_err = std::string("cudaMallocAsync: ") + cudaGetErrorString(e);
@@ -572,7 +604,9 @@ size_t scratch_budget_doubles() {
 
 // Schwarz ordering (index_sort + find_threshold) and the active pair arrays.
 int build_active(hfgpu_handle* h) {
-    HF_DEVICE_LOCK;
+    // no library lock here: the allocations are stream-ordered, and holding
+    // the lock across this function's stream synchronisations made the jobs
+    // of a server queue behind one another's GPU work
     for (int t = 0; t < NPT; ++t) {
         int n = (int)h->pairs[t].size();
         h->schw[t].resize(n);
@@ -969,7 +1003,6 @@ extern "C" {
 const char* hfgpu_last_error(void) { return g_err.c_str(); }
 
 int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
-    HF_DEVICE_LOCK;
     if (!B || !out || B->nsh <= 0 || B->nb <= 0 || B->maxprim <= 0)
         return set_err(HFGPU_ERR_ARG, "hfgpu_init: bad arguments");
     *out = nullptr;
@@ -1045,23 +1078,17 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
         hfgpu_finalize(h);
         return HFGPU_ERR_NOMEM;
     }
-    // the buffers are ready for the synchronous uploads below once the
-    // handle's stream has run the allocations
-    ce = cudaStreamSynchronize(h->stream);
-    if (ce != cudaSuccess) {
-        std::string m = std::string("hfgpu_init: ") + cudaGetErrorString(ce);
-        hfgpu_finalize(h);
-        return set_err(HFGPU_ERR_CUDA, m);
-    }
     for (int i = 0; i < 2 * NCLS + 2; ++i) cudaEventCreate(&h->ev[i]);
     cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming);
     for (int k = 0; k < NSTREAM; ++k) {
         cudaStreamCreateWithFlags(&h->aux[k], cudaStreamNonBlocking);
         cudaEventCreateWithFlags(&h->join[k], cudaEventDisableTiming);
     }
+    // uploads on the handle's own stream (pageable sources are staged before
+    // the call returns); one synchronisation of that stream at the end
     auto up = [&](void* d, const void* s, size_t bytes) {
         if (bytes == 0) return cudaSuccess;
-        return cudaMemcpy(d, s, bytes, cudaMemcpyHostToDevice);
+        return cudaMemcpyAsync(d, s, bytes, cudaMemcpyHostToDevice, h->stream);
     };
     ce = up(h->d_shtyp, h->shtyp.data(), h->nsh * sizeof(int));
     if (ce == cudaSuccess) ce = up(h->d_aosh, h->aosh.data(), h->nsh * sizeof(int));
@@ -1133,7 +1160,6 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
 
 int hfgpu_finalize(hfgpu_handle* h) {
     if (!h) return HFGPU_OK;
-    HF_DEVICE_LOCK;
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->gexec) cudaGraphExecDestroy(h->gexec);
     if (h->graph) cudaGraphDestroy(h->graph);

@@ -457,6 +457,7 @@ thread_local std::string g_onee_err;
 
 namespace hfgpu {
 void set_last_error(const std::string& msg);  // hfgpu.cu
+cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t st);  // hfgpu.cu: the library's memory pool
 }
 
 namespace {
@@ -466,7 +467,7 @@ namespace {
 // copy before it returns.
 template <typename T>
 cudaError_t up(T** d, const std::vector<T>& h, cudaStream_t st) {
-    cudaError_t e = cudaMallocAsync((void**)d, std::max<size_t>(h.size(), 1) * sizeof(T), st);
+    cudaError_t e = hfgpu::pool_alloc((void**)d, std::max<size_t>(h.size(), 1) * sizeof(T), st);
     if (e == cudaSuccess && !h.empty())
         e = cudaMemcpyAsync(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st);
     return e;
@@ -576,7 +577,7 @@ extern "C" int hfgpu_one_electron_gpu(const hfgpu_basis* B, int natom, const dou
     if (e == cudaSuccess) e = up(&d_ch, ch, st);
     if (e == cudaSuccess) e = up(&d_xyz, xz, st);
     const size_t nb2 = (size_t)nb * nb;
-    if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_out, 3 * nb2 * sizeof(double), st);
+    if (e == cudaSuccess) e = hfgpu::pool_alloc((void**)&d_out, 3 * nb2 * sizeof(double), st);
     if (e == cudaSuccess) {
         g.pairs = d_pairs; g.pcls = d_pcls; g.npairs = (int)sp.size(); g.cls = d_cls; g.ops = d_ops;
         g.targets = d_targets; g.shtyp = d_shtyp; g.nzet = d_nzet; g.aosh = d_aosh; g.xsh = d_xsh;

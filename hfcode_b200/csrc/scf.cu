@@ -28,6 +28,7 @@
 namespace hfgpu {
 void set_last_error(const std::string& msg);
 std::recursive_mutex& device_mutex();
+cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t st);  // the library's memory pool
 }  // namespace hfgpu
 
 namespace {
@@ -411,7 +412,7 @@ int create(hfgpu_handle* h, int nocc, double enuc, const double* S, const double
     const size_t o_w = take(nb * sizeof(double)), o_info = take(sizeof(int)), o_sc = take(sizeof(CycleScalars));
     const size_t o_aux = take((4 + 2 * (size_t)nb) * sizeof(double)), o_ws = take(ws);
     const size_t o_work = take((size_t)std::max(1, s->lwork) * sizeof(double));
-    SCF_CUDA(cudaMallocAsync(&s->arena, off, s->st));
+    SCF_CUDA(hfgpu::pool_alloc(&s->arena, off, s->st));
     char* base = (char*)s->arena;
     for (int k = 0; k < 13; ++k) *mats[k] = (double*)(base + o_mats[k]);
     for (int k = 0; k < NDIIS; ++k) {

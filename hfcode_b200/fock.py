@@ -42,11 +42,11 @@ class HfgpuError(RuntimeError):
     pass
 
 
-# CUDA forbids device-synchronising calls (cudaFree, ...) in one thread while
-# another records a stream capture.  The library serialises its own captures
-# and allocations; callers that record their own graphs around library calls
-# (device_scf) hold this lock while recording, and handle creation, the
-# Schwarz pass (which sizes buffers) and release take it too.
+# A stream capture in global mode forbids device-synchronising calls
+# (cudaFree, ...) in every thread.  The library allocates stream-ordered and
+# records its own captures in thread-local mode, so its calls need no lock;
+# callers that record their own graphs around library calls (device_scf)
+# hold this lock while recording, for their own framework's sake.
 DEVICE_LOCK = threading.RLock()
 
 
@@ -160,16 +160,14 @@ class FockBuilder:
         self.nsh = shells.nsh
         self._desc = BasisDescriptor(shells)
         h = ctypes.c_void_p()
-        with DEVICE_LOCK:
-            _check(_lib.hfgpu_init(ctypes.addressof(self._desc.struct), ctypes.byref(h)), "hfgpu_init")
+        _check(_lib.hfgpu_init(ctypes.addressof(self._desc.struct), ctypes.byref(h)), "hfgpu_init")
         self.h = h
         if scratch_budget is not None:
             self.set_scratch_budget(scratch_budget)
 
     def close(self):
         if getattr(self, "h", None):
-            with DEVICE_LOCK:
-                _lib.hfgpu_finalize(self.h)
+            _lib.hfgpu_finalize(self.h)
             self.h = None
 
     def __del__(self):
@@ -189,8 +187,7 @@ class FockBuilder:
     # --- the reference's entry points -------------------------------------
     def fock_build_initial_diag(self, f: np.ndarray, p: np.ndarray, thr: float):
         fp, pp, keep = self._fp(f, p)
-        with DEVICE_LOCK:
-            _check(_lib.hfgpu_fock_build_initial_diag(self.h, fp, pp, float(thr)), "fock_build_initial_diag")
+        _check(_lib.hfgpu_fock_build_initial_diag(self.h, fp, pp, float(thr)), "fock_build_initial_diag")
 
     def fock_build_diag(self, f: np.ndarray, p: np.ndarray, thr: float):
         fp, pp, keep = self._fp(f, p)
