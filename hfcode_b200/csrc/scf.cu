@@ -3,11 +3,11 @@
 // memory and the cycle driven from C++ on the builder handle's stream.
 //
 //   Fock builds        this library (device-pointer entry points of hfgpu.h)
-//   E_elec, DIIS rows  cuBLAS ddot into device scalars
+//   E_elec, DIIS rows  one pass over the matrices (k_cycle_scalars) into device scalars
 //   F P S - S P F, X^T R X, X F X^T, C = X C', P = 2 C_occ C_occ^T   cuBLAS dgemm/geam
 //   the density        SP2 purification (cuBLAS dgemm); cuSOLVER syevd where
 //                      eigenvectors are needed (core guess, level shift, orbital energies)
-//   max |R|, max |dP|  one reduction kernel
+//   max |R|, max |dP|  the same pass
 //
 // The host reads one small block of scalars per cycle (two dots, the new
 // DIIS row, two maxima) and takes the protocol's decisions as the reference
@@ -43,19 +43,6 @@ struct CycleScalars {
     unsigned long long resmax;     // max |R| as the bits of a non-negative double
     unsigned long long dpmax;      // max |P - Pold|
 };
-
-// max |a - b| (b may be null: max |a|) over n values into *out; the bit
-// patterns of non-negative doubles order like the values, so an integer
-// atomicMax combines the blocks.
-__global__ void k_absmax(const double* __restrict__ a, const double* __restrict__ b, size_t n,
-                         unsigned long long* out) {
-    double m = 0.0;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        m = fmax(m, fabs(b ? a[i] - b[i] : a[i]));
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
-}
 
 // out[:, j] = v[:, j] / sqrt(w[j]) (columns of an n x n column-major matrix)
 __global__ void k_scale_cols(const double* __restrict__ v, const double* __restrict__ w, double* __restrict__ out,
@@ -109,49 +96,114 @@ __global__ void k_gershgorin_bounds(const double* __restrict__ lo, const double*
     }
 }
 
-// X = (hi I - F) / (hi - lo): the start of the purification, spectrum in [0, 1]
-// with the occupied orbitals (lowest energies) nearest 1
-__global__ void k_sp2_start(const double* __restrict__ f, const double* __restrict__ bounds, double* __restrict__ x,
-                            int n) {
-    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-    if (t >= (size_t)n * n) return;
-    const double lo = bounds[0], hi = bounds[1];
-    const int i = (int)(t % n), j = (int)(t / n);
-    x[t] = ((i == j ? hi : 0.0) - f[t]) / (hi - lo);
+// Block sums of two values into acc[0], acc[1] with one atomic each.
+__device__ __forceinline__ void block_add2(double a, double b, double* acc) {
+    __shared__ double sa[32], sb[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    if (lane == 0) {
+        sa[w] = a;
+        sb[w] = b;
+    }
+    __syncthreads();
+    if (w == 0) {
+        a = lane < nw ? sa[lane] : 0.0;
+        b = lane < nw ? sb[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, o);
+            b += __shfl_xor_sync(0xffffffffu, b, o);
+        }
+        if (lane == 0) {
+            atomicAdd(acc, a);
+            atomicAdd(acc + 1, b);
+        }
+    }
 }
 
-// traces of X and X^2 into tr[0], tr[1] (one block)
-__global__ void k_traces(const double* __restrict__ x, const double* __restrict__ x2, int n, double* tr) {
-    __shared__ double s1[256], s2[256];
-    double a = 0.0, b = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        a += x[i + (size_t)i * n];
-        b += x2[i + (size_t)i * n];
+// X = (hi I - F) / (hi - lo): the start of the purification, spectrum in [0, 1]
+// with the occupied orbitals (lowest energies) nearest 1.  Adds tr X and
+// ||X||_F^2 (= tr X^2, X symmetric) into tr[0], tr[1] (zeroed before).
+__global__ void k_sp2_start(const double* __restrict__ f, const double* __restrict__ bounds, double* __restrict__ x,
+                            int n, double* tr) {
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    double d = 0.0, q = 0.0;
+    if (t < (size_t)n * n) {
+        const double lo = bounds[0], hi = bounds[1];
+        const int i = (int)(t % n), j = (int)(t / n);
+        const double v = ((i == j ? hi : 0.0) - f[t]) / (hi - lo);
+        x[t] = v;
+        d = i == j ? v : 0.0;
+        q = v * v;
     }
-    s1[threadIdx.x] = a;
-    s2[threadIdx.x] = b;
-    __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if (threadIdx.x < o) {
-            s1[threadIdx.x] += s1[threadIdx.x + o];
-            s2[threadIdx.x] += s2[threadIdx.x + o];
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        tr[0] = s1[0];
-        tr[1] = s2[0];
-    }
+    block_add2(d, q, tr);
 }
 
 // One SP2 step: X <- X^2 when that brings the trace nearer nocc, else
-// X <- 2X - X^2 (trace of 2X - X^2 is 2 tr X - tr X^2).
-__global__ void k_sp2_step(double* __restrict__ x, const double* __restrict__ x2, const double* __restrict__ tr,
-                           double nocc, size_t n2) {
+// X <- 2X - X^2 (tr(2X - X^2) = 2 tr X - tr X^2), decided from tr_in (tr X,
+// tr X^2 of the current X).  Adds the new X's traces into tr_out and clears
+// tr_clear, the slot the next step adds into.
+__global__ void k_sp2_update(double* __restrict__ x, const double* __restrict__ x2, const double* __restrict__ tr_in,
+                             double* tr_out, double* tr_clear, double nocc, int n) {
     const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-    if (t >= n2) return;
-    const bool square = fabs(tr[1] - nocc) < fabs(2.0 * tr[0] - tr[1] - nocc);
-    x[t] = square ? x2[t] : 2.0 * x[t] - x2[t];
+    if (t == 0) {
+        tr_clear[0] = 0.0;
+        tr_clear[1] = 0.0;
+    }
+    double d = 0.0, q = 0.0;
+    if (t < (size_t)n * n) {
+        const bool square = fabs(tr_in[1] - nocc) < fabs(2.0 * tr_in[0] - tr_in[1] - nocc);
+        const double v = square ? x2[t] : 2.0 * x[t] - x2[t];
+        x[t] = v;
+        d = (t % n) == (t / n) ? v : 0.0;
+        q = v * v;
+    }
+    block_add2(d, q, tr_out);
+}
+
+// The cycle's scalars in one pass: sum P H, sum P F, <R_new, R_j> for the
+// eight history slots, max |R_new| and max |P - Pold|, into out (zeroed).
+struct CycleArgs {
+    const double* P;
+    const double* H;
+    const double* F;
+    const double* R;
+    const double* Rj[8];
+    const double* Pold;
+    size_t n;
+};
+__global__ void k_cycle_scalars(CycleArgs c, CycleScalars* out) {
+    double ph = 0.0, pf = 0.0, br[8] = {}, rm = 0.0, dm = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < c.n; i += (size_t)gridDim.x * blockDim.x) {
+        const double p = c.P[i], r = c.R[i];
+        ph += p * c.H[i];
+        pf += p * c.F[i];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) br[k] += r * c.Rj[k][i];
+        rm = fmax(rm, fabs(r));
+        dm = fmax(dm, fabs(p - c.Pold[i]));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        ph += __shfl_xor_sync(0xffffffffu, ph, o);
+        pf += __shfl_xor_sync(0xffffffffu, pf, o);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) br[k] += __shfl_xor_sync(0xffffffffu, br[k], o);
+        rm = fmax(rm, __shfl_xor_sync(0xffffffffu, rm, o));
+        dm = fmax(dm, __shfl_xor_sync(0xffffffffu, dm, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&out->ph, ph);
+        atomicAdd(&out->pf, pf);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) atomicAdd(&out->brow[k], br[k]);
+        atomicMax(&out->resmax, (unsigned long long)__double_as_longlong(rm));
+        atomicMax(&out->dpmax, (unsigned long long)__double_as_longlong(dm));
+    }
 }
 
 int fail(int code, const std::string& msg) {
@@ -180,7 +232,7 @@ struct hfgpu_scf {
     void* blas_ws = nullptr;
     void* arena = nullptr;       // one stream-ordered allocation holding every buffer above
     CycleScalars* sc = nullptr;  // device
-    double* aux = nullptr;       // purification: bounds[2], traces[2], then row bounds lo[nb], hi[nb]
+    double* aux = nullptr;       // purification: bounds[2], trace slots[6], then row bounds lo[nb], hi[nb]
     bool eigs_current = false;   // W/eigs describe the last Fob
     size_t bytes = 0;
     // protocol state, carried from one hfgpu_scf_run call to the next
@@ -276,26 +328,30 @@ int density_by_purification(hfgpu_scf* s, const double* Fo, double* P) {
     double* X = s->T1;
     double* X2 = s->T2;
     double* bounds = s->aux;
-    double* tr = s->aux + 2;
-    k_gershgorin_rows<<<(unsigned)((nb + 7) / 8), 256, 0, s->st>>>(Fo, nb, s->aux + 4, s->aux + 4 + nb);
-    k_gershgorin_bounds<<<1, 1024, 0, s->st>>>(s->aux + 4, s->aux + 4 + nb, nb, bounds);
-    k_sp2_start<<<blocks, 256, 0, s->st>>>(Fo, bounds, X, nb);
+    double* tr = s->aux + 2;  // three slots of (tr X, tr X^2), rotating with the steps
+    double* lo = s->aux + 8;
+    k_gershgorin_rows<<<(unsigned)((nb + 7) / 8), 256, 0, s->st>>>(Fo, nb, lo, lo + nb);
+    k_gershgorin_bounds<<<1, 1024, 0, s->st>>>(lo, lo + nb, nb, bounds);
+    SCF_CUDA(cudaMemsetAsync(tr, 0, 6 * sizeof(double), s->st));
+    k_sp2_start<<<blocks, 256, 0, s->st>>>(Fo, bounds, X, nb, tr);
     SCF_CUDA(cudaGetLastError());
     // the first check after 16 steps (the start needs ~log2 of the spectral
-    // range over the gap of them), then every 4
+    // range over the gap of them), then every 4; each step is the product X^2
+    // and one update kernel that also forms the next step's traces
     constexpr int FIRST = 16, BLOCK = 4, MAXSTEP = 160;
     for (int step = 0; step < MAXSTEP;) {
         const int nstep = step == 0 ? FIRST : BLOCK;
         for (int k = 0; k < nstep; ++k) {
+            const int q = step + k;
             SCF_RC(gemm(s, false, false, 1.0, X, X, 0.0, X2));
-            k_traces<<<1, 256, 0, s->st>>>(X, X2, nb, tr);
-            k_sp2_step<<<blocks, 256, 0, s->st>>>(X, X2, tr, (double)s->nocc, n2);
+            k_sp2_update<<<blocks, 256, 0, s->st>>>(X, X2, tr + 2 * (q % 3), tr + 2 * ((q + 1) % 3),
+                                                    tr + 2 * ((q + 2) % 3), (double)s->nocc, nb);
         }
         step += nstep;
         s->sp2_steps += nstep;
         SCF_CUDA(cudaGetLastError());
         double h_tr[2];
-        SCF_CUDA(cudaMemcpyAsync(h_tr, tr, sizeof(h_tr), cudaMemcpyDeviceToHost, s->st));
+        SCF_CUDA(cudaMemcpyAsync(h_tr, tr + 2 * (step % 3), sizeof(h_tr), cudaMemcpyDeviceToHost, s->st));
         SCF_CUDA(cudaStreamSynchronize(s->st));
         // tr X - tr X^2 = sum x_k (1 - x_k) over the eigenvalues: zero for a projector
         if (std::fabs(h_tr[0] - h_tr[1]) < 1e-11 * std::max(1, s->nocc)) break;
@@ -410,7 +466,7 @@ int create(hfgpu_handle* h, int nocc, double enuc, const double* S, const double
         o_fo[k] = take(bytes);
     }
     const size_t o_w = take(nb * sizeof(double)), o_info = take(sizeof(int)), o_sc = take(sizeof(CycleScalars));
-    const size_t o_aux = take((4 + 2 * (size_t)nb) * sizeof(double)), o_ws = take(ws);
+    const size_t o_aux = take((8 + 2 * (size_t)nb) * sizeof(double)), o_ws = take(ws);
     const size_t o_work = take((size_t)std::max(1, s->lwork) * sizeof(double));
     SCF_CUDA(hfgpu::pool_alloc(&s->arena, off, s->st));
     char* base = (char*)s->arena;
@@ -538,15 +594,18 @@ int run(hfgpu_scf* s, const hfgpu_scf_params& prm, hfgpu_scf_result* res) {
         SCF_RC(gemm(s, false, false, 1.0, s->T2, s->X, 0.0, s->R[fresh]));
         SCF_RC(copy(s, s->FO[fresh], s->Fob));
         // the cycle's scalars
-        SCF_CUDA(cudaMemsetAsync(&s->sc->resmax, 0, 2 * sizeof(unsigned long long), s->st));
-        SCF_BLAS(cublasSetPointerMode(s->blas, CUBLAS_POINTER_MODE_DEVICE));
-        SCF_BLAS(cublasDdot(s->blas, (int)n2, s->P, 1, s->H, 1, &s->sc->ph));
-        SCF_BLAS(cublasDdot(s->blas, (int)n2, s->P, 1, s->F, 1, &s->sc->pf));
-        for (int k = 0; k < NDIIS; ++k)
-            SCF_BLAS(cublasDdot(s->blas, (int)n2, s->R[fresh], 1, s->R[slot[k]], 1, &s->sc->brow[k]));
-        SCF_BLAS(cublasSetPointerMode(s->blas, CUBLAS_POINTER_MODE_HOST));
-        k_absmax<<<grid, 256, 0, s->st>>>(s->R[fresh], nullptr, n2, &s->sc->resmax);
-        k_absmax<<<grid, 256, 0, s->st>>>(s->P, s->Pold, n2, &s->sc->dpmax);
+        SCF_CUDA(cudaMemsetAsync(s->sc, 0, sizeof(CycleScalars), s->st));
+        {
+            CycleArgs ca{};
+            ca.P = s->P;
+            ca.H = s->H;
+            ca.F = s->F;
+            ca.R = s->R[fresh];
+            for (int k = 0; k < NDIIS; ++k) ca.Rj[k] = s->R[slot[k]];
+            ca.Pold = s->Pold;
+            ca.n = n2;
+            k_cycle_scalars<<<grid, 256, 0, s->st>>>(ca, s->sc);
+        }
         SCF_CUDA(cudaGetLastError());
         CycleScalars cs;
         SCF_CUDA(cudaMemcpyAsync(&cs, s->sc, sizeof(cs), cudaMemcpyDeviceToHost, s->st));
