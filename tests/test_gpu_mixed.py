@@ -5,7 +5,7 @@ the Fock matrix and the converged energy stay close to FP64.  Stated
 tolerances: max|dF| <= 1e-5 for an all-FP32 off-diagonal build (every
 quartet in FP32, a stress case well beyond any cutoff) on a perturbed density
 of benzene, and |dE| <= 1e-6 Eh for the SCF with the mixed
-incremental builds (the north-star target), which in practice lands far
+incremental builds (the mixed form's accuracy target), which in practice lands far
 below it."""
 import json
 import os
