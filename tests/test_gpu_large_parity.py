@@ -116,3 +116,37 @@ def test_c20h42_mixed_form():
     assert de <= 1e-6
     assert st["fp32"].sum() > 0
     assert df < 1e-6
+
+
+@pytest.mark.gpu
+def test_c20h42_j_only_and_incremental_builds_match_oracle():
+    """n-C20H42 against the oracle run here: the Coulomb-only build
+    (fock_build_non_diag_j.f90) at the core-guess density, and an
+    incremental build (direct_hartreefock.f90:111-121: fock_build_diag at
+    thr, fock_build_non_diag at thr*0.1) on the difference of the two
+    guesses; 1e-10 element-wise, equal screened-in counts."""
+    from hfcode_b200.fock import FockBuilder
+    from oracle import pyoracle
+    fx = np.load(os.path.join(GOLD, "fock_c20h42.npz"))
+    _, _, sh, p_sad = system("alkane20")
+    nb = sh.nb
+    p_core = untri(fx["P_core"], nb)
+    fb, orc = FockBuilder(sh), pyoracle.Oracle(sh)
+    for obj in (fb, orc):
+        obj.fock_build_initial_diag(np.zeros((nb, nb)), p_sad, 1e-10)
+    jg, jo = np.zeros((nb, nb)), np.zeros((nb, nb))
+    fb.fock_build_non_diag_j_only(jg, p_core, 1e-10)
+    orc.fock_build_non_diag_j_only(jo, p_core, 1e-10)
+    assert np.max(np.abs(jg - jo)) < FTOL
+    dp = p_core - p_sad
+    dg, do = np.zeros((nb, nb)), np.zeros((nb, nb))
+    fb.fock_build_diag(dg, dp, 1e-10)
+    orc.fock_build_diag(do, dp, 1e-10)
+    fb.fock_build_non_diag(dg, dp, 1e-11)
+    orc.fock_build_non_diag(do, dp, 1e-11)
+    counts = fb.class_stats()["pass"]
+    fb.close()
+    err = float(np.max(np.abs(dg - do)))
+    print(f"c20h42 incremental build: max|dF_gpu - dF_oracle| = {err:.2e}")
+    assert err < FTOL
+    assert np.array_equal(counts, counts_by_gpu_class(orc.counts()[0]))
