@@ -544,6 +544,214 @@ __global__ void __launch_bounds__(ND_THREADS, sizeof(E) == 4 ? 3 : 2) k_scatter_
     if (a.stats) warp_add_stats(a.stats, nsc, npr, a.f32 ? nsc : 0ull);
 }
 
+// ------------------------------------- grouped staged scatter (4 lanes) ----
+// One quartet per group of SG = 4 lanes.  Lane g owns function g of one bra
+// shell O (S = 0: the first bra shell a, S = 1: the second, b), which has
+// four functions; X is the other bra shell.  The lane reads the rows of its
+// NX slabs (o = g, x = 0..NX-1), each NC*ND rows, and forms
+//   complete over the quartet:  J_OX[g][x] (P_cd), K_Oc[g][k] (P_Xd), K_Od[g][l] (P_Xc)
+//   summed over the group:      K_Xc[x][k] (P_Od), K_Xd[x][l] (P_Oc) after slab x,
+//                               J_cd[k][l] (P_OX) after the last slab
+// Group sums are two-step reduce-scatters (xor 1, xor 2), so each lane adds a
+// quarter of them and a quartet still issues one atomic per block element.
+// Against the one-thread scatter a thread holds about a third of the block
+// sums, which leaves room for more warps per SM to hide the latency of the
+// row and density loads.
+constexpr int SG = 4;
+__host__ __device__ constexpr int scatg_smem_bytes(int NX, int NC, int ND, int es) {
+    // two slab buffers of NC*ND rows per thread, then P_cd, P_Xc and P_Xd of
+    // each quartet of the block ([value][quartet])
+    return 2 * NC * ND * ND_THREADS * es + (NC * ND + NX * (NC + ND)) * (ND_THREADS / SG) * es;
+}
+// blocks per SM: as many as the shared memory allows, at most SCATG_BLK64
+// for FP64 sums and four for FP32 sums (128 registers)
+#ifndef SCATG_BLK64
+#define SCATG_BLK64 3
+#endif
+__host__ __device__ constexpr int scatg_cap(int es) { return es == 8 ? SCATG_BLK64 : 4; }
+__host__ __device__ constexpr int scatg_minb(int NX, int NC, int ND, int es) {
+    return 225 * 1024 / scatg_smem_bytes(NX, NC, ND, es) < scatg_cap(es) ? 225 * 1024 / scatg_smem_bytes(NX, NC, ND, es)
+                                                                         : scatg_cap(es);
+}
+
+// Sum N values over the four lanes of a group (reduce-scatter): on return
+// v[0 .. N/4) hold the group sums of elements base .. base + N/4 of the
+// input, base = (g&1 ? N/2 : 0) + (g&2 ? N/4 : 0).  N is a multiple of 4.
+template <int N, typename E>
+__device__ __forceinline__ int group_reduce_scatter(E* v, int g) {
+    constexpr int H1 = N / 2, H2 = N / 4;
+    const bool b0 = g & 1, b1 = g & 2;
+#pragma unroll
+    for (int i = 0; i < H1; ++i) {
+        const E lo = v[i], hi = v[H1 + i];
+        v[i] = (b0 ? hi : lo) + __shfl_xor_sync(0xffffffffu, b0 ? lo : hi, 1);
+    }
+#pragma unroll
+    for (int i = 0; i < H2; ++i) {
+        const E lo = v[i], hi = v[H2 + i];
+        v[i] = (b1 ? hi : lo) + __shfl_xor_sync(0xffffffffu, b1 ? lo : hi, 2);
+    }
+    return (b0 ? H1 : 0) + (b1 ? H2 : 0);
+}
+
+template <int NA, int NB, int NC, int ND, int S, typename E = double>
+__global__ void __launch_bounds__(ND_THREADS, scatg_minb(S == 0 ? NB : NA, NC, ND, (int)sizeof(E)))
+    k_scatter_grouped(StagedArgs a) {
+    constexpr int T = ND_THREADS, QB = T / SG, SLAB = NC * ND, NBUF = 2;
+    constexpr int NO = S == 0 ? NA : NB, NX = S == 0 ? NB : NA;
+    static_assert(NO == SG, "the lane-owned shell has four functions");
+    constexpr int NK = NC + ND, NK4 = (NK + 3) / 4 * 4;  // K_Xc[x], K_Xd[x] of one slab
+    constexpr int NJ4 = (NC * ND + 3) / 4 * 4;           // J_cd
+    constexpr int NPS = NC * ND + NX * NK;               // density values in shared memory
+    const int tid = threadIdx.x, lane = tid & 31, g = tid & (SG - 1), ql = tid / SG;
+    const int cnt = staged_count(a);
+    const int qi = blockIdx.x * QB + ql;
+    const int w0 = blockIdx.x * QB + (tid - lane) / SG;  // first quartet of this warp
+    if (w0 >= cnt) return;                              // whole warps only
+    // a group past the end works on the warp's first quartet and writes nothing
+    const bool valid = qi < cnt;
+    const int tq = valid ? qi : w0;
+    double mxq = 0.0;
+    for (int r = 0; r < a.nroles; ++r) mxq = fmax(mxq, a.mx[(size_t)r * a.stride + tq]);
+    const uint2 q = staged_quartet(a, tq);
+    const GPair bra = a.bra[q.x];
+    const GPair ket = a.ket[q.y];
+    const bool act = valid && !(mxq < a.thr);  // fock_build_non_diag.f90:69
+    const bool jonly = a.jonly != 0;
+    const int nsh = a.nsh;
+    const int sO = S == 0 ? bra.sa : bra.sb, sX = S == 0 ? bra.sb : bra.sa;
+    const int O0 = S == 0 ? bra.aoa : bra.aob, X0 = S == 0 ? bra.aob : bra.aoa;
+    const int c0 = ket.aoa, d0 = ket.aob;
+    // density blocks in shell-pair order, row-major within a block
+    const double* __restrict__ Pb = a.Pb;
+    const double* __restrict__ Bab = Pb + __ldg(a.boff + bra.sa * nsh + bra.sb);
+    const double* __restrict__ BOc = Pb + __ldg(a.boff + sO * nsh + ket.sa);
+    const double* __restrict__ BOd = Pb + __ldg(a.boff + sO * nsh + ket.sb);
+    const double* __restrict__ BXc = Pb + __ldg(a.boff + sX * nsh + ket.sa);
+    const double* __restrict__ BXd = Pb + __ldg(a.boff + sX * nsh + ket.sb);
+    const double* __restrict__ Bcd = Pb + __ldg(a.boff + ket.sa * nsh + ket.sb);
+    extern __shared__ __align__(16) double hf_scatg_smem[];
+    E* eb = reinterpret_cast<E*>(hf_scatg_smem) + tid;                 // [NBUF][SLAB][T], own column
+    E* sp = reinterpret_cast<E*>(hf_scatg_smem) + NBUF * SLAB * T + ql;  // [NPS][QB]: P_cd, P_Xc, P_Xd
+    const E* __restrict__ e = reinterpret_cast<const E*>(a.out) + tq;
+    const size_t st = a.stride;
+    auto issue = [&](int x) {
+        if (x < NX) {
+            const E* src = e + (size_t)((S == 0 ? g * NB + x : x * NB + g) * SLAB) * st;
+            E* dst = eb + (x % NBUF) * SLAB * T;
+#pragma unroll
+            for (int r = 0; r < SLAB; ++r) cp_async_elem(dst + r * T, src + (size_t)r * st);
+        }
+        cp_async_commit();  // empty groups keep the count uniform
+    };
+    issue(0);
+    // the quartet's P_cd, P_Xc and P_Xd, loaded once by its four lanes
+    for (int v = g; v < NPS; v += SG)
+        sp[v * QB] = (E)__ldg(v < SLAB ? Bcd + v : v < SLAB + NX * NC ? BXc + (v - SLAB) : BXd + (v - SLAB - NX * NC));
+    E poc[NC], pod[ND], pox[NX];
+#pragma unroll
+    for (int k = 0; k < NC; ++k) poc[k] = (E)__ldg(BOc + g * NC + k);
+#pragma unroll
+    for (int l = 0; l < ND; ++l) pod[l] = (E)__ldg(BOd + g * ND + l);
+#pragma unroll
+    for (int x = 0; x < NX; ++x) pox[x] = (E)__ldg(Bab + (S == 0 ? g * NB + x : x * NB + g));
+    __syncwarp();
+    // warp-uniform shells: a block element with one address for the whole
+    // warp is summed over the warp's eight quartets and added by one lane
+    auto same = [](int x) { return __all_sync(0xffffffffu, x == __shfl_sync(0xffffffffu, x, 0)); };
+    const bool ua = same(bra.aoa), ub = same(bra.aob), uc = same(c0), ud = same(d0);
+    const bool uO = S == 0 ? ua : ub, uX = S == 0 ? ub : ua;
+    auto Ga = [&](int r, int c) { return a.G + r + (size_t)c * a.nb; };
+    // `shuf` is warp-uniform (every lane runs the shuffles); `uni` may differ
+    // between lanes of different g but is the same for lanes of equal g,
+    // which are the lanes the shuffles sum over
+    auto emit = [&](double* addr, double v, bool shuf, bool uni, bool has) {
+        double r = v;
+        if (shuf) {
+            r += __shfl_xor_sync(0xffffffffu, r, 4);
+            r += __shfl_xor_sync(0xffffffffu, r, 8);
+            r += __shfl_xor_sync(0xffffffffu, r, 16);
+        }
+        if (uni) {
+            if (lane < SG && has) atomicAdd(addr, r);
+        } else if (act && has) {
+            atomicAdd(addr, v);
+        }
+    };
+    const double s = (bra.sa == bra.sb ? 0.5 : 1.0) * (ket.sa == ket.sb ? 0.5 : 1.0);
+    const double s2 = 2.0 * s, hs = -0.5 * s;
+    E koc[NC], kod[ND], jcd[NJ4];
+#pragma unroll
+    for (int k = 0; k < NC; ++k) koc[k] = 0;
+#pragma unroll
+    for (int l = 0; l < ND; ++l) kod[l] = 0;
+#pragma unroll
+    for (int v = 0; v < NJ4; ++v) jcd[v] = 0;
+#pragma unroll
+    for (int x = 0; x < NX; ++x) {
+        issue(x + 1);
+        cp_async_wait<NBUF - 1>();  // this thread's copies of slab x have landed
+        const E* es = eb + (x % NBUF) * SLAB * T;
+        E pxd[ND], kx[NK4], jox = 0;
+#pragma unroll
+        for (int l = 0; l < ND; ++l) pxd[l] = sp[(SLAB + NX * NC + x * ND + l) * QB];
+#pragma unroll
+        for (int v = 0; v < NK4; ++v) kx[v] = 0;
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+            const E pxc = sp[(SLAB + x * NC + k) * QB];
+#pragma unroll
+            for (int l = 0; l < ND; ++l) {
+                const E v = es[(k * ND + l) * T];
+                jox += sp[(k * ND + l) * QB] * v;
+                jcd[k * ND + l] += pox[x] * v;
+                if (!jonly) {
+                    koc[k] += pxd[l] * v;
+                    kod[l] += pxc * v;
+                    kx[k] += pod[l] * v;       // K_Xc[x][k]
+                    kx[NC + l] += poc[k] * v;  // K_Xd[x][l]
+                }
+            }
+        }
+        emit(S == 0 ? Ga(O0 + g, X0 + x) : Ga(X0 + x, O0 + g), act ? s2 * (double)jox : 0.0, ua && ub, ua && ub,
+             true);
+        if (!jonly) {
+            const int base = group_reduce_scatter<NK4>(kx, g);
+            const bool shuf = uX && (uc || ud);  // warp-uniform
+#pragma unroll
+            for (int v = 0; v < NK4 / 4; ++v) {
+                const int y = base + v;
+                const bool isc = y < NC;
+                emit(Ga(X0 + x, isc ? c0 + y : d0 + (y - NC)), act && y < NK ? hs * (double)kx[v] : 0.0, shuf,
+                     uX && (isc ? uc : ud), y < NK);
+            }
+        }
+    }
+    cp_async_wait<0>();
+    if (!jonly) {
+#pragma unroll
+        for (int k = 0; k < NC; ++k)
+            emit(Ga(O0 + g, c0 + k), act ? hs * (double)koc[k] : 0.0, uO && uc, uO && uc, true);
+#pragma unroll
+        for (int l = 0; l < ND; ++l)
+            emit(Ga(O0 + g, d0 + l), act ? hs * (double)kod[l] : 0.0, uO && ud, uO && ud, true);
+    }
+    {
+        const int base = group_reduce_scatter<NJ4>(jcd, g);
+#pragma unroll
+        for (int v = 0; v < NJ4 / 4; ++v) {
+            const int y = base + v;
+            emit(Ga(c0 + y / ND, d0 + y % ND), act && y < NC * ND ? s2 * (double)jcd[v] : 0.0, uc && ud, uc && ud,
+                 y < NC * ND);
+        }
+    }
+    if (a.stats) {  // counted once per quartet, by its lane 0
+        const unsigned long long nsc = act && g == 0 ? 1ull : 0ull;
+        const unsigned long long npr = valid && g == 0 ? (unsigned long long)(bra.np * ket.np) : 0ull;
+        warp_add_stats(a.stats, nsc, npr, a.f32 ? nsc : 0ull);
+    }
+}
+
 // Diagonal builders of a staged class (quartets (ab|ab), one per pair):
 // MODE 0 writes the Schwarz factor sqrt(max|e|) (fock_build_initial_diag),
 // MODE 1 applies the density screen schw^2 max(D_ab, D_aa/4, D_bb/4) < thr
@@ -598,6 +806,11 @@ struct ClassKernels {
     int scat_smem;                // dynamic shared memory of scat (bytes)
     StagedKernel scat32;          // scatter of FP32 chunks (float rows), or nullptr
     int scat32_smem;
+    // grouped scatter (four lanes per quartet) where a bra shell has four
+    // functions, else nullptr
+    StagedKernel scatg, scatg32;
+    int scatg_smem, scatg32_smem;
+    int grp64, grp32;             // the grouped scatter is the default for FP64 / FP32 chunks
     // every role of a stage in one launch (gridDim.y = roles), for small chunks
     StagedKernel ma64, ma32;      // stage-A roles (staged3)
     StagedKernel mb64, mb32;      // output / HRR roles

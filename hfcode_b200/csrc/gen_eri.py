@@ -606,6 +606,7 @@ def class_params(tag: str) -> dict:
     prm.setdefault("acc_max32", 2 * prm["acc_max"])
     prm.setdefault("acc_group32", 2 * prm["acc_group"])
     prm.setdefault("out_max32", 2 * prm["out_max"])
+    prm.setdefault("minb32", 2)  # blocks per SM of the FP32 output-role kernels (staged2)
     return prm
 
 
@@ -642,6 +643,25 @@ __global__ void __launch_bounds__(ND_THREADS, {minb}) {kname}(StagedArgs a) {{
         default: break;
     }}
 }}"""
+
+
+def grouped_scatter_reg(NA: int, NB: int, NC: int, ND: int, prm: dict) -> str:
+    """Registration of the grouped scatter (four lanes per quartet, lane g
+    owning function g of a four-function bra shell: the first shell when it
+    has four functions, else the second), or nullptr when neither has.
+    scat_grouped64 / scat_grouped32 in the tuning table choose it by default
+    for the FP64 / FP32 chunks of the class (measured per class)."""
+    S = 0 if NA == 4 else 1 if NB == 4 else -1
+    if S < 0:
+        return ("    k->scatg = nullptr;\n    k->scatg32 = nullptr;\n"
+                "    k->scatg_smem = 0;\n    k->scatg32_smem = 0;\n    k->grp64 = 0;\n    k->grp32 = 0;")
+    NX = NB if S == 0 else NA
+    return (f"    k->scatg = k_scatter_grouped<{NA}, {NB}, {NC}, {ND}, {S}>;\n"
+            f"    k->scatg_smem = scatg_smem_bytes({NX}, {NC}, {ND}, 8);\n"
+            f"    k->scatg32 = k_scatter_grouped<{NA}, {NB}, {NC}, {ND}, {S}, float>;\n"
+            f"    k->scatg32_smem = scatg_smem_bytes({NX}, {NC}, {ND}, 4);\n"
+            f"    k->grp64 = {int(bool(prm.get('scat_grouped64', False)))};\n"
+            f"    k->grp32 = {int(bool(prm.get('scat_grouped32', False)))};")
 
 
 def class_source(ci: int, bi: int, ki: int):
@@ -711,7 +731,7 @@ __device__ __forceinline__ void {kname}_body(const StagedArgs& a) {{
 {stores}
     a.mx[(size_t){r} * a.stride + t] = mx;
 }}
-__global__ void __launch_bounds__(ND_THREADS, 2) {kname}(StagedArgs a) {{ {kname}_body(a); }}"""
+__global__ void __launch_bounds__(ND_THREADS, {prm["minb32"] if f32 else 2}) {kname}(StagedArgs a) {{ {kname}_body(a); }}"""
 
         for r, outs in enumerate(roles):
             code, _ = g.emit_role(f"{g.name}_r{r}", outs)
@@ -734,6 +754,7 @@ __global__ void __launch_bounds__(ND_THREADS, 2) {kname}(StagedArgs a) {{ {kname
                    f"    k->scat_smem = scat_smem_bytes({NA}, {NB}, {NC}, {ND});\n"
                    f"    k->scat32 = k_scatter_staged<{NA}, {NB}, {NC}, {ND}, float>;\n"
                    f"    k->scat32_smem = scat_smem_bytes({NA}, {NB}, {NC}, {ND}, 4);")
+        reg.append(grouped_scatter_reg(NA, NB, NC, ND, prm))
         if bi == ki:
             reg.append(f"    k->diag0 = nullptr;\n    k->diag1 = nullptr;")
             reg.append(f"    k->dscat0 = k_scatter_diag<{NA}, {NB}, 0>;\n    k->dscat1 = k_scatter_diag<{NA}, {NB}, 1>;")
@@ -809,6 +830,7 @@ __global__ void __launch_bounds__(ND_THREADS) {kname}(StagedArgs a) {{ {kname}_b
                    f"    k->scat_smem = scat_smem_bytes({NA}, {NB}, {NC}, {ND});\n"
                    f"    k->scat32 = k_scatter_staged<{NA}, {NB}, {NC}, {ND}, float>;\n"
                    f"    k->scat32_smem = scat_smem_bytes({NA}, {NB}, {NC}, {ND}, 4);")
+        reg.append(grouped_scatter_reg(NA, NB, NC, ND, prm))
         if bi == ki:
             reg.append(f"    k->diag0 = nullptr;\n    k->diag1 = nullptr;")
             reg.append(f"    k->dscat0 = k_scatter_diag<{NA}, {NB}, 0>;\n    k->dscat1 = k_scatter_diag<{NA}, {NB}, 1>;")

@@ -327,6 +327,7 @@ struct hfgpu_handle {
     int timing = 0;
     int device = 0;                       // the CUDA device current at hfgpu_init
     long long merge_blocks = 0;           // chunks up to this many role blocks run one launch per stage
+    int grouped_scatter = 1;              // four-lane scatter: 1 per class tuning, 2 everywhere, 0 nowhere
     cudaStream_t stream = nullptr;
     cudaStream_t aux[NSTREAM] = {};    // independent classes run concurrently on these
     cudaEvent_t fork = nullptr, join[NSTREAM] = {};
@@ -448,6 +449,10 @@ struct ClassTable {
                 cudaFuncSetAttribute(k[c].scat, cudaFuncAttributeMaxDynamicSharedMemorySize, k[c].scat_smem);
             if (k[c].scat32 && k[c].scat32_smem > 0)
                 cudaFuncSetAttribute(k[c].scat32, cudaFuncAttributeMaxDynamicSharedMemorySize, k[c].scat32_smem);
+            if (k[c].scatg && k[c].scatg_smem > 0)
+                cudaFuncSetAttribute(k[c].scatg, cudaFuncAttributeMaxDynamicSharedMemorySize, k[c].scatg_smem);
+            if (k[c].scatg32 && k[c].scatg32_smem > 0)
+                cudaFuncSetAttribute(k[c].scatg32, cudaFuncAttributeMaxDynamicSharedMemorySize, k[c].scatg32_smem);
         }
     }
 };
@@ -854,8 +859,18 @@ int run_staged(hfgpu_handle* h, int c, int prec, long long n, const double* P, d
             }
         }
         ++h->launches;
-        if (prec && K.scat32) K.scat32<<<blocks, ND_THREADS, K.scat32_smem, stream>>>(a);  // float rows
-        else K.scat<<<blocks, ND_THREADS, K.scat_smem, stream>>>(a);
+        // grouped scatter: where the class's tuning chooses it (grouped_scatter 1),
+        // everywhere it exists (2) or nowhere (0)
+        const bool grp = h->grouped_scatter == 2 || (h->grouped_scatter == 1 && (prec ? K.grp32 : K.grp64));
+        const StagedKernel sg = grp ? (prec ? K.scatg32 : K.scatg) : nullptr;
+        if (sg) {  // four lanes per quartet
+            const int gblocks = (int)(((long long)m * SG + ND_THREADS - 1) / ND_THREADS);
+            sg<<<gblocks, ND_THREADS, prec ? K.scatg32_smem : K.scatg_smem, stream>>>(a);
+        } else if (prec && K.scat32) {
+            K.scat32<<<blocks, ND_THREADS, K.scat32_smem, stream>>>(a);  // float rows
+        } else {
+            K.scat<<<blocks, ND_THREADS, K.scat_smem, stream>>>(a);
+        }
         HF_CHECK(cudaGetLastError());
     }
     return HFGPU_OK;
@@ -1047,6 +1062,8 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
         // 10.8 jobs/s without merging, 14.9 at 2 x SMs, 23.9 at 8 x SMs
         h->merge_blocks = 8LL * h->nsm;
         if (const char* e = getenv("HFGPU_MERGE_BLOCKS")) h->merge_blocks = atoll(e);
+        if (const char* e = getenv("HFGPU_SCATTER"))  // "single" / "grouped" override the per-class choice
+            h->grouped_scatter = strcmp(e, "single") == 0 ? 0 : strcmp(e, "grouped") == 0 ? 2 : 1;
     }
     int rc = 0;
     const size_t nb2 = (size_t)h->nb * h->nb;
