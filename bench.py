@@ -445,7 +445,11 @@ def run_reference(args):
                       "e2e": {"value": v, "unit": "builds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
-LLDL_DRAM_BYTES_PER_QUARTET = 2805.0  # (130.1 + 3647.0 MB read + 33.4 MB written) / 5 builds / 271,664 quartets
+# DRAM bytes per LL|DL quartet of one C60 build (role kernels + scatter),
+# from one ncu capture of this benchmark's own command (five builds, caches
+# left as the program uses them): (281.0 GB read + 273.4 GB written) / 5 builds
+# / 20,498,336 quartets
+LLDL_DRAM_BYTES_PER_QUARTET = 5408.0
 
 
 def main():
@@ -545,8 +549,7 @@ def main():
     achieved = cls_flops[top] / (st["ms"][top] * 1e-3) / 1e12
     peak_tf = fp64_peak / 1e3
     # DRAM bytes per LL|DL quartet (role kernels + scatter) from one ncu
-    # capture of these same kernels on n-C30H62 (271,664 LL|DL quartets per
-    # build), scaled by this build's LL|DL quartet count
+    # capture of this command on C60, times this build's LL|DL quartet count
     traffic = None
     if fock.CLASS_NAMES[top] == "LL|DL":
         traffic = LLDL_DRAM_BYTES_PER_QUARTET * float(st["pass"][top])
@@ -566,8 +569,9 @@ def main():
     roof = {"bound": "fp64", "kernel": f"class {fock.CLASS_NAMES[top]} (role kernels + k_scatter_staged)",
             "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf,
             "traffic": traffic, "traffic_unit": "bytes per build of the class",
-            "traffic_source": "scaled: 2805 DRAM bytes per LL|DL quartet (role kernels + scatter) measured by ncu on "
-                              "n-C30H62 with these kernels, times this build's LL|DL quartet count",
+            "traffic_source": "ncu capture of this C60 command (dram__bytes_read.sum + dram__bytes_write.sum of "
+                              "the LL|DL role kernels and scatter, five builds): 5408 bytes per LL|DL quartet, "
+                              "times this build's LL|DL quartet count",
             "hbm_view": hbm_view,
             "peak_source": "measured FP64 FMA-chain probe on this device (MEASURED_PEAKS.json has no FP64 figure)",
             "all_classes_tflops": float(cls_flops.sum() / (st["ms"].sum() * 1e-3) / 1e12),
