@@ -208,3 +208,45 @@ def test_merged_and_separate_role_launches_agree(name):
             os.environ["HFGPU_MERGE_BLOCKS"] = old
     assert np.max(np.abs(out["separate"][0] - out["merged"][0])) < 1e-11
     assert out["merged"][1] < out["separate"][1]  # fewer launches
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["benzene", "alkane2_mix"])
+def test_grouped_and_single_thread_scatter_agree(name):
+    """The staged scatter runs one thread per quartet, or four lanes per
+    quartet where the class's tuning chooses it; HFGPU_SCATTER at handle
+    creation forces one form everywhere.  FP64 builds and mixed builds (FP32
+    chunks below the cutoff) of both forms agree to rounding, and the FP64
+    builds match the oracle."""
+    import os
+    from hfcode_b200.fock import FockBuilder
+    _, _, sh, p0 = system(name)
+    nb = sh.nb
+    p = perturbed_density(p0, 10)
+    out = {}
+    old = os.environ.get("HFGPU_SCATTER")
+    try:
+        for mode in ("single", "grouped"):
+            os.environ["HFGPU_SCATTER"] = mode
+            fb = FockBuilder(sh)
+            f64 = np.zeros((nb, nb))
+            fb.fock_build_initial_diag(f64, p0, 1e-10)
+            fb.fock_build_non_diag(f64, p, 1e-10)
+            fmx = np.zeros((nb, nb))
+            fb.fock_build_non_diag_mixed(fmx, p, 1e-10, 1e3)  # every quartet in FP32
+            out[mode] = (f64, fmx)
+            fb.close()
+    finally:
+        if old is None:
+            os.environ.pop("HFGPU_SCATTER", None)
+        else:
+            os.environ["HFGPU_SCATTER"] = old
+    orc = pyoracle.Oracle(sh)
+    fo = np.zeros((nb, nb), order="F")
+    orc.fock_build_initial_diag(fo, p0, 1e-10)
+    orc.fock_build_non_diag(fo, p, 1e-10)
+    assert np.max(np.abs(out["single"][0] - out["grouped"][0])) < 1e-12
+    assert np.max(np.abs(out["grouped"][0] - fo)) < 1e-10
+    # FP32 block sums: the two forms add the same FP32 products in different orders
+    scale = max(1.0, float(np.max(np.abs(out["single"][1]))))
+    assert np.max(np.abs(out["single"][1] - out["grouped"][1])) < 1e-5 * scale
