@@ -308,7 +308,7 @@ struct StagedArgs {
     double* acc;
     double* out;
     double* mx;
-    size_t stride;         // columns of the scratch rows (chunk capacity)
+    size_t stride;         // chunk capacity in quartets (a multiple of the tile size TQ)
     int nroles;            // rows of mx
     const double* P;
     double* G;
@@ -333,14 +333,24 @@ __device__ __forceinline__ int staged_count(const StagedArgs& a) {
     return (int)(left < 0 ? 0 : left < a.n ? left : a.n);
 }
 
+// Scratch layout of a chunk.  Each region (accumulators, outputs, role
+// maxima) is a sequence of tiles of TQ quartets; a tile holds the region's R
+// rows of its quartets, row-major: element (row, t) sits at
+// tcol(t, R) + row * TQ.  A block of ND_THREADS = TQ threads then reads and
+// writes one contiguous span of R * TQ elements (a few hundred KB, within
+// one or two pages), instead of R rows as far apart as the chunk is long.
+constexpr int TQ = 128;
+static_assert(TQ == ND_THREADS, "a block of the staged kernels covers one scratch tile");
+__device__ __forceinline__ size_t tcol(int t, int R) { return (size_t)(t / TQ) * R * TQ + (t % TQ); }
+
 __device__ __forceinline__ uint2 staged_quartet(const StagedArgs& a, int t) {
     const long long i = a.q0 + t + (a.ncls && a.prec ? (long long)a.ncls[2 * a.cls] : 0);
     return a.quartets[i];
 }
 
 // ------------------------------------------- staged scatter, async loads ----
-// The staged scatter reads each quartet's ERI block (one column of the
-// scratch rows) once.  With ~255 registers per thread only 8 warps fit on an
+// The staged scatter reads each quartet's ERI block (its column of the
+// chunk's output tile) once.  With ~255 registers per thread only 8 warps fit on an
 // SM, too few to hide the latency of plain loads, so the block's rows are
 // streamed into shared memory with per-thread cp.async copies: slab s (the
 // NC*ND rows of one (i, j)) is consumed while slabs s+1 .. s+NBUF-1 are in
@@ -530,7 +540,8 @@ __global__ void __launch_bounds__(ND_THREADS, sizeof(E) == 4 ? 3 : 2) k_scatter_
     const bool valid = t < cnt;
     const int tq = valid ? t : w0;
     double m = 0.0;
-    for (int r = 0; r < a.nroles; ++r) m = fmax(m, a.mx[(size_t)r * a.stride + tq]);
+    const double* __restrict__ mxc = a.mx + tcol(tq, a.nroles);
+    for (int r = 0; r < a.nroles; ++r) m = fmax(m, mxc[r * TQ]);
     const uint2 q = staged_quartet(a, tq);
     const GPair bra = a.bra[q.x];
     const GPair ket = a.ket[q.y];
@@ -539,7 +550,8 @@ __global__ void __launch_bounds__(ND_THREADS, sizeof(E) == 4 ? 3 : 2) k_scatter_
     const unsigned long long npr = valid ? (unsigned long long)(bra.np * ket.np) : 0ull;
     const double s = (bra.sa == bra.sb ? 0.5 : 1.0) * (ket.sa == ket.sb ? 0.5 : 1.0);
     extern __shared__ __align__(16) double hf_scat_smem[];
-    scatter_async<NA, NB, NC, ND, E>(reinterpret_cast<const E*>(a.out) + tq, a.stride, s, bra, ket, a.Pb, a.boff,
+    scatter_async<NA, NB, NC, ND, E>(reinterpret_cast<const E*>(a.out) + tcol(tq, NA * NB * NC * ND), TQ, s, bra,
+                                     ket, a.Pb, a.boff,
                                      a.nsh, a.G, a.nb, a.jonly != 0, act, reinterpret_cast<E*>(hf_scat_smem));
     if (a.stats) warp_add_stats(a.stats, nsc, npr, a.f32 ? nsc : 0ull);
 }
@@ -612,7 +624,8 @@ __global__ void __launch_bounds__(ND_THREADS, scatg_minb(S == 0 ? NB : NA, NC, N
     const bool valid = qi < cnt;
     const int tq = valid ? qi : w0;
     double mxq = 0.0;
-    for (int r = 0; r < a.nroles; ++r) mxq = fmax(mxq, a.mx[(size_t)r * a.stride + tq]);
+    const double* __restrict__ mxc = a.mx + tcol(tq, a.nroles);
+    for (int r = 0; r < a.nroles; ++r) mxq = fmax(mxq, mxc[r * TQ]);
     const uint2 q = staged_quartet(a, tq);
     const GPair bra = a.bra[q.x];
     const GPair ket = a.ket[q.y];
@@ -633,8 +646,8 @@ __global__ void __launch_bounds__(ND_THREADS, scatg_minb(S == 0 ? NB : NA, NC, N
     extern __shared__ __align__(16) double hf_scatg_smem[];
     E* eb = reinterpret_cast<E*>(hf_scatg_smem) + tid;                 // [NBUF][SLAB][T], own column
     E* sp = reinterpret_cast<E*>(hf_scatg_smem) + NBUF * SLAB * T + ql;  // [NPS][QB]: P_cd, P_Xc, P_Xd
-    const E* __restrict__ e = reinterpret_cast<const E*>(a.out) + tq;
-    const size_t st = a.stride;
+    const E* __restrict__ e = reinterpret_cast<const E*>(a.out) + tcol(tq, NA * NB * NC * ND);
+    const size_t st = TQ;
     auto issue = [&](int x) {
         if (x < NX) {
             const E* src = e + (size_t)((S == 0 ? g * NB + x : x * NB + g) * SLAB) * st;
@@ -765,7 +778,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_scatter_diag(StagedArgs a) {
     const GPair pr = a.bra[q.x];
     if (MODE == 0) {
         double m = 0.0;
-        for (int r = 0; r < a.nroles; ++r) m = fmax(m, a.mx[(size_t)r * a.stride + t]);
+        for (int r = 0; r < a.nroles; ++r) m = fmax(m, a.mx[tcol(t, a.nroles) + r * TQ]);
         a.schw[q.x] = sqrt(m);
     } else {
         const double mv = fmax(a.md[pr.sa * a.nsh + pr.sb],
@@ -773,14 +786,14 @@ __global__ void __launch_bounds__(ND_THREADS) k_scatter_diag(StagedArgs a) {
         const double sw = a.schw[q.x];
         if (sw * sw * mv < a.thr) return;
     }
-    double* e = a.out + t;
+    double* e = a.out + tcol(t, NA * NB * NA * NB);
 #pragma unroll 1
     for (int i = 0; i < NA * NB * NA * NB; ++i) {
-        const double v = e[(size_t)i * a.stride];
-        if (!(fabs(v) > INTTHRESH)) e[(size_t)i * a.stride] = 0.0;  // element skip
+        const double v = e[(size_t)i * TQ];
+        if (!(fabs(v) > INTTHRESH)) e[(size_t)i * TQ] = 0.0;  // element skip
     }
     const double f = pr.sa == pr.sb ? 1.0 : 2.0;
-    scatter_strided<NA, NB, NA, NB>(e, a.stride, f * f / 8.0, pr, pr, a.P, a.G, a.nb, false);
+    scatter_strided<NA, NB, NA, NB>(e, TQ, f * f / 8.0, pr, pr, a.P, a.G, a.nb, false);
 }
 
 typedef void (*NDKernel)(NDArgs);

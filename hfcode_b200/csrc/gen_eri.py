@@ -708,9 +708,12 @@ def class_source(ci: int, bi: int, ki: int):
         # twice the size, so fewer of them repeat the primitive loop
         roles32 = g.partition(prm["acc_max32"], prm["out_max32"])
 
+        def nroles_of(f32):  # rows of the role maxima of a chunk of this precision
+            return len(roles32) if f32 else len(roles)
+
         def s2_kernel(kname, fname, outs, r, f32):
             real = "float" if f32 else "double"
-            stores = "\n".join(f"    {{ const double v = (double)e[{i}]; out[(size_t){n} * a.stride + t] = ({real})v; "
+            stores = "\n".join(f"    {{ const double v = (double)e[{i}]; out[{n} * TQ] = ({real})v; "
                                f"mx = fmax(mx, fabs(v)); }}" for i, n in enumerate(outs))
             tab = "a.boysf" if f32 else "a.boys"
             return f"""
@@ -727,9 +730,10 @@ __device__ __forceinline__ void {kname}_body(const StagedArgs& a) {{
     {real} e[{len(outs)}];
     {fname}(bra, ket, a.prims, sboys, e);
     double mx = 0.0;
-    {real}* out = reinterpret_cast<{real}*>(a.out);  // FP32 chunks keep FP32 rows
+    // this quartet's column of the chunk's output tile (FP32 chunks keep FP32 rows)
+    {real}* out = reinterpret_cast<{real}*>(a.out) + tcol(t, {g.nout});
 {stores}
-    a.mx[(size_t){r} * a.stride + t] = mx;
+    a.mx[tcol(t, {nroles_of(f32)}) + {r} * TQ] = mx;
 }}
 __global__ void __launch_bounds__(ND_THREADS, {prm["minb32"] if f32 else 2}) {kname}(StagedArgs a) {{ {kname}_body(a); }}"""
 
@@ -787,7 +791,7 @@ __device__ __forceinline__ void {kpre}_{g.tag}_r{r}_body(const StagedArgs& a) {{
     const uint2 q = staged_quartet(a, t);
     const GPair bra = a.bra[q.x];
     const GPair ket = a.ket[q.y];
-    {fname}(bra, ket, a.prims, sboys, reinterpret_cast<{real}*>(a.acc) + (size_t){base} * a.stride + t, a.stride);
+    {fname}(bra, ket, a.prims, sboys, reinterpret_cast<{real}*>(a.acc) + tcol(t, {len(keyidx)}) + {base} * TQ, TQ);
 }}
 __global__ void __launch_bounds__(ND_THREADS, 2) {kpre}_{g.tag}_r{r}(StagedArgs a) {{ {kpre}_{g.tag}_r{r}_body(a); }}""")
                 base += len(gr)
@@ -806,9 +810,9 @@ __device__ __forceinline__ void {kname}_body(const StagedArgs& a) {{
     const uint2 q = staged_quartet(a, t);
     const GPair bra = a.bra[q.x];
     const GPair ket = a.ket[q.y];
-    a.mx[(size_t){r} * a.stride + t] =
-        {fname}(bra, ket, reinterpret_cast<const {real}*>(a.acc) + t,
-                reinterpret_cast<{real}*>(a.out) + (size_t){outs[0]} * a.stride + t, a.stride);
+    a.mx[tcol(t, {len(outroles)}) + {r} * TQ] =
+        {fname}(bra, ket, reinterpret_cast<const {real}*>(a.acc) + tcol(t, {len(keyidx)}),
+                reinterpret_cast<{real}*>(a.out) + tcol(t, {g.nout}) + {outs[0]} * TQ, TQ);
 }}
 __global__ void __launch_bounds__(ND_THREADS) {kname}(StagedArgs a) {{ {kname}_body(a); }}""")
         kern.append(merged_kernel(f"k_sam_{g.tag}", [f"k_sa_{g.tag}_r{r}" for r in range(len(groups))]))

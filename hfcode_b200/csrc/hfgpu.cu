@@ -783,7 +783,7 @@ int build_active(hfgpu_handle* h) {
         if (K.mode == 0 || h->ccap[c] == 0) continue;
         const size_t per = (size_t)K.nacc + K.nout + std::max(K.nrole_b, K.nrole_b32);
         size_t st = std::min<size_t>((size_t)h->ccap[c], budget / per);
-        st = std::max<size_t>(st, 128);
+        st = (std::max<size_t>(st, TQ) + TQ - 1) / TQ * TQ;  // whole scratch tiles
         h->stride[c] = st;
         need = std::max(need, st * per);
     }
@@ -1220,7 +1220,7 @@ static int alloc_diag_scratch(hfgpu_handle* h) {
         const size_t n = h->pairs[t].size();
         if (K.mode == 0 || n == 0) continue;
         const size_t per = (size_t)K.nacc + K.nout + K.nrole_b;
-        const size_t st = std::max<size_t>(std::min<size_t>(n, budget / per), 128);
+        const size_t st = (std::max<size_t>(std::min<size_t>(n, budget / per), TQ) + TQ - 1) / TQ * TQ;  // whole tiles
         h->dstride[t] = st;
         need = std::max(need, st * per);
     }
