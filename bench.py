@@ -447,9 +447,9 @@ def run_reference(args):
 
 # DRAM bytes per LL|DL quartet of one C60 build (role kernels + scatter),
 # from one ncu capture of this benchmark's own command (five builds, caches
-# left as the program uses them): (281.0 GB read + 273.4 GB written) / 5 builds
+# left as the program uses them): (280.5 GB read + 273.0 GB written) / 5 builds
 # / 20,498,336 quartets
-LLDL_DRAM_BYTES_PER_QUARTET = 5408.0
+LLDL_DRAM_BYTES_PER_QUARTET = 5401.0
 
 
 def main():
@@ -570,7 +570,7 @@ def main():
             "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf,
             "traffic": traffic, "traffic_unit": "bytes per build of the class",
             "traffic_source": "ncu capture of this C60 command (dram__bytes_read.sum + dram__bytes_write.sum of "
-                              "the LL|DL role kernels and scatter, five builds): 5408 bytes per LL|DL quartet, "
+                              "the LL|DL role kernels and scatter, five builds): 5401 bytes per LL|DL quartet, "
                               "times this build's LL|DL quartet count",
             "hbm_view": hbm_view,
             "peak_source": "measured FP64 FMA-chain probe on this device (MEASURED_PEAKS.json has no FP64 figure)",
