@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(ND_THREADS) k_diag(DiagArgs a) {
 
 // Arguments of the staged classes' kernels: a chunk of the class's quartet
 // list, and the scratch it goes through (accumulators, outputs and the
-// per-role maxima, each [row][stride] with one column per quartet).
+// per-role maxima, each in tiles of TQ quartets: see tcol below).
 struct StagedArgs {
     const uint2* quartets;
     int n;                 // quartets in this chunk (an upper bound when ncls is set)
