@@ -858,66 +858,6 @@ __global__ void __launch_bounds__(ND_THREADS) {kname}(StagedArgs a) {{ {kname}_b
     return cuh, cu, info
 
 
-def role_kernels(g: "ClassGen", roles, diag: bool, diag_only: bool = False) -> str:
-    """Diagonal-builder kernels of a class split into R roles: a block is R
-    warps over 32 shell pairs; warp r evaluates role r of the pair of its
-    lane, and the Schwarz max is reduced across the warps through shared
-    memory."""
-    R = len(roles)
-    nmax = max(len(x) for x in roles)
-    tag, L = g.tag, g.L
-    dcases = []
-    for r, outs in enumerate(roles):
-        dcases.append(f"        case {r}: eri_{tag}_r{r}(pr, pr, a.prims, sboys, e); nloc = {len(outs)}; break;")
-    return f"""
-template <int MODE>
-__global__ void __launch_bounds__({32 * R}) k_dg_{tag}(DiagArgs a) {{
-    __shared__ double sboys[BOYS_BLK];
-    __shared__ double smax[{32 * R}];
-    stage_boys<{L}>(sboys, a.boys);
-    const int lane = threadIdx.x & 31, role = threadIdx.x >> 5;
-    const int t = blockIdx.x * 32 + lane;
-    bool valid = t < a.n;
-    const GPair pr = a.pairs[valid ? t : 0];
-    if (MODE == 1 && valid) {{
-        const double mv = fmax(a.md[pr.sa * a.nsh + pr.sb],
-                               fmax(0.25 * a.md[pr.sb * a.nsh + pr.sb], 0.25 * a.md[pr.sa * a.nsh + pr.sa]));
-        const double sw = a.schw[t];
-        if (sw * sw * mv < a.thr) valid = false;  // fock_build_diag.f90:20-21
-    }}
-    double e[{nmax}];
-    int nloc = 0;
-    double mx = 0.0;
-    if (valid) {{
-        switch (role) {{
-{chr(10).join(dcases)}
-        }}
-#pragma unroll
-        for (int i = 0; i < {nmax}; ++i)
-            if (i < nloc) mx = fmax(mx, fabs(e[i]));
-    }}
-    smax[threadIdx.x] = mx;
-    __syncthreads();
-    if (MODE == 0 && valid && role == 0) {{
-        double g = 0.0;
-#pragma unroll
-        for (int r = 0; r < {R}; ++r) g = fmax(g, smax[r * 32 + lane]);
-        a.schw[t] = sqrt(g);
-    }}
-    if (valid) {{
-#pragma unroll
-        for (int i = 0; i < {nmax}; ++i)
-            if (!(fabs(e[i]) > INTTHRESH)) e[i] = 0.0;  // element skip
-        const double f = pr.sa == pr.sb ? 1.0 : 2.0;
-        const double s = f * f / 8.0;
-        switch (role) {{
-{chr(10).join(f"            case {r}: scat_{tag}_r{r}(e, s, pr, pr, a.P, a.G, a.nb, false); break;" for r in range(R))}
-        }}
-    }}
-}}
-"""
-
-
 CLASS_CUH = """// GENERATED by gen_eri.py -- do not edit.
 // Device functions of quartet class ({A}{B}|{C}{D}): {roles} role(s).
 #pragma once
