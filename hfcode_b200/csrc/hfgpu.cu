@@ -114,7 +114,7 @@ namespace {
     } while (0)
 
 constexpr double SHTHRESH = 1e-11;      // molprops.f90:163
-constexpr int NSTREAM = 4;              // concurrent class streams of the off-diagonal build
+constexpr int NSTREAM = 8;              // class streams a handle creates (HFGPU_STREAMS of them used, default 4)
 // bra and ket pair types of the 21 quartet classes (pair types i <= j, row by row)
 __constant__ int CLS_BI[NCLS] = {HF_CLASS_BI_LIST};
 __constant__ int CLS_KI[NCLS] = {HF_CLASS_KI_LIST};
@@ -328,6 +328,7 @@ struct hfgpu_handle {
     int device = 0;                       // the CUDA device current at hfgpu_init
     long long merge_blocks = 0;           // chunks up to this many role blocks run one launch per stage
     int grouped_scatter = 1;              // four-lane scatter: 1 per class tuning, 2 everywhere, 0 nowhere
+    int nstreams = 4;                     // class streams the off-diagonal build uses (<= NSTREAM)
     cudaStream_t stream = nullptr;
     cudaStream_t aux[NSTREAM] = {};    // independent classes run concurrently on these
     cudaEvent_t fork = nullptr, join[NSTREAM] = {};
@@ -799,7 +800,7 @@ int build_active(hfgpu_handle* h) {
     // (accumulators + outputs + role maxima) doubles per quartet
     size_t need = 0;
     const size_t budget = (h->scratch_budget ? h->scratch_budget / sizeof(double) : scratch_budget_doubles()) /
-                          NSTREAM;  // one slot per class stream
+                          h->nstreams;  // one slot per class stream
     for (int c = 0; c < NCLS; ++c) {
         const ClassKernels& K = CLASS_KERNELS[c];
         h->stride[c] = 0;
@@ -810,12 +811,12 @@ int build_active(hfgpu_handle* h) {
         h->stride[c] = st;
         need = std::max(need, st * per);
     }
-    if (need * NSTREAM > h->scratch_doubles) {
+    if (need * h->nstreams > h->scratch_doubles) {
         dfree(h->d_scratch, h->stream);
         h->scratch_doubles = 0;
-        int rc = dalloc(&h->d_scratch, need * NSTREAM, h->stream);
+        int rc = dalloc(&h->d_scratch, need * h->nstreams, h->stream);
         if (rc) return rc;
-        h->scratch_doubles = need * NSTREAM;
+        h->scratch_doubles = need * h->nstreams;
     }
     h->slot_doubles = need;
     h->have_schwarz = true;
@@ -900,7 +901,7 @@ int run_staged(hfgpu_handle* h, int c, int prec, long long n, const double* P, d
 }
 
 // Off-diagonal build: the two screening passes with device-side offsets,
-// then the class kernels on NSTREAM concurrent streams.  With capture set,
+// then the class kernels on the handle's concurrent class streams.  With capture set,
 // nothing is read back on the host: every launch is sized by the class's
 // candidate count (an upper bound) and the kernels read the surviving count
 // from d_ncls, so the whole sequence can be recorded into a CUDA graph.
@@ -958,7 +959,7 @@ int run_non_diag(hfgpu_handle* h, const double* P, double thr, int jonly, double
             h->n32[c] = (long long)cnt[2 * c + 1];
         }
     }
-    // work items (class, precision) over NSTREAM concurrent streams, largest
+    // work items (class, precision) over the class streams, largest
     // first onto the least-loaded stream; with timing on, everything runs in
     // order on the handle's stream
     struct Item { int c, prec; long long n; double w; };
@@ -975,7 +976,7 @@ int run_non_diag(hfgpu_handle* h, const double* P, double thr, int jonly, double
     if (multi) {
         std::stable_sort(items.begin(), items.end(), [](const Item& x, const Item& y) { return x.w > y.w; });
         HF_CHECK(cudaEventRecord(h->fork, h->stream));
-        for (int k = 0; k < NSTREAM; ++k) HF_CHECK(cudaStreamWaitEvent(h->aux[k], h->fork, 0));
+        for (int k = 0; k < h->nstreams; ++k) HF_CHECK(cudaStreamWaitEvent(h->aux[k], h->fork, 0));
     }
     double load[NSTREAM] = {};
     for (const Item& it : items) {
@@ -983,7 +984,7 @@ int run_non_diag(hfgpu_handle* h, const double* P, double thr, int jonly, double
         const long long n = it.n;
         const ClassKernels& K = CLASS_KERNELS[c];
         int k = 0;
-        for (int q = 1; q < NSTREAM; ++q)
+        for (int q = 1; q < h->nstreams; ++q)
             if (load[q] < load[k]) k = q;
         load[k] += it.w;
         cudaStream_t st = multi ? h->aux[k] : h->stream;
@@ -1026,7 +1027,7 @@ int run_non_diag(hfgpu_handle* h, const double* P, double thr, int jonly, double
         }
     }
     if (multi) {
-        for (int k = 0; k < NSTREAM; ++k) {
+        for (int k = 0; k < h->nstreams; ++k) {
             HF_CHECK(cudaEventRecord(h->join[k], h->aux[k]));
             HF_CHECK(cudaStreamWaitEvent(h->stream, h->join[k], 0));
         }
@@ -1085,6 +1086,7 @@ int hfgpu_init(const hfgpu_basis* B, hfgpu_handle** out) {
         // 10.8 jobs/s without merging, 14.9 at 2 x SMs, 23.9 at 8 x SMs
         h->merge_blocks = 8LL * h->nsm;
         if (const char* e = getenv("HFGPU_MERGE_BLOCKS")) h->merge_blocks = atoll(e);
+        if (const char* e = getenv("HFGPU_STREAMS")) h->nstreams = std::max(1, std::min(NSTREAM, atoi(e)));
         if (const char* e = getenv("HFGPU_SCATTER"))  // "single" / "grouped" override the per-class choice
             h->grouped_scatter = strcmp(e, "single") == 0 ? 0 : strcmp(e, "grouped") == 0 ? 2 : 1;
     }
