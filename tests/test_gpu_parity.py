@@ -250,3 +250,37 @@ def test_grouped_and_single_thread_scatter_agree(name):
     # FP32 block sums: the two forms add the same FP32 products in different orders
     scale = max(1.0, float(np.max(np.abs(out["single"][1]))))
     assert np.max(np.abs(out["single"][1] - out["grouped"][1])) < 1e-5 * scale
+
+
+@pytest.mark.gpu
+def test_class_stream_count_does_not_change_f():
+    """HFGPU_STREAMS (read at handle creation) spreads the classes over one to
+    eight concurrent streams, each with its own scratch slot.  The F of one
+    and of eight streams agree to rounding and match the oracle."""
+    import os
+    from hfcode_b200.fock import FockBuilder
+    _, _, sh, p0 = system("alkane2_mix")
+    nb = sh.nb
+    p = perturbed_density(p0, 11)
+    out = {}
+    old = os.environ.get("HFGPU_STREAMS")
+    try:
+        for n in ("1", "8"):
+            os.environ["HFGPU_STREAMS"] = n
+            fb = FockBuilder(sh)
+            f = np.zeros((nb, nb))
+            fb.fock_build_initial_diag(f, p0, 1e-10)
+            fb.fock_build_non_diag(f, p, 1e-10)
+            out[n] = f
+            fb.close()
+    finally:
+        if old is None:
+            os.environ.pop("HFGPU_STREAMS", None)
+        else:
+            os.environ["HFGPU_STREAMS"] = old
+    orc = pyoracle.Oracle(sh)
+    fo = np.zeros((nb, nb), order="F")
+    orc.fock_build_initial_diag(fo, p0, 1e-10)
+    orc.fock_build_non_diag(fo, p, 1e-10)
+    assert np.max(np.abs(out["1"] - out["8"])) < 1e-12
+    assert np.max(np.abs(out["8"] - fo)) < 1e-10
