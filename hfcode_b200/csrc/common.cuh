@@ -204,6 +204,16 @@ __device__ __forceinline__ void warp_add_stats(ClassStats* st, unsigned long lon
 }
 
 constexpr int ND_THREADS = 128;
+// Threads per block of the staged role kernels, a divisor of ND_THREADS.
+// Smaller blocks at the same registers per thread (more blocks per SM) let
+// the role kernels of one class stream and the scatters of another share
+// the SMs at a finer grain.  C60 FP64 build: 197.6 ms with 128 threads,
+// 194.1 with 64, 192.7 with 32; all-FP32 build 124.8, 122.3, 122.3 ms.
+#ifndef HF_RB_THREADS
+#define HF_RB_THREADS 32
+#endif
+constexpr int RB_THREADS = HF_RB_THREADS, RB_SCALE = ND_THREADS / RB_THREADS;
+static_assert(RB_THREADS * RB_SCALE == ND_THREADS, "role blocks tile a scratch tile exactly");
 
 template <class C, bool F32>
 __global__ void __launch_bounds__(ND_THREADS) k_nondiag(NDArgs a) {

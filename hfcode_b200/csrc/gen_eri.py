@@ -637,7 +637,7 @@ def merged_kernel(kname: str, bodies: List[str], minb: int = 2) -> str:
     launches themselves would set the time."""
     cases = "\n".join(f"        case {r}: {b}_body(a); break;" for r, b in enumerate(bodies))
     return f"""
-__global__ void __launch_bounds__(ND_THREADS, {minb}) {kname}(StagedArgs a) {{
+__global__ void __launch_bounds__(RB_THREADS, {minb} * RB_SCALE) {kname}(StagedArgs a) {{
     switch (blockIdx.y) {{
 {cases}
         default: break;
@@ -735,7 +735,7 @@ __device__ __forceinline__ void {kname}_body(const StagedArgs& a) {{
 {stores}
     a.mx[tcol(t, {nroles_of(f32)}) + {r} * TQ] = mx;
 }}
-__global__ void __launch_bounds__(ND_THREADS, {prm["minb32"] if f32 else 2}) {kname}(StagedArgs a) {{ {kname}_body(a); }}"""
+__global__ void __launch_bounds__(RB_THREADS, {prm["minb32"] if f32 else 2} * RB_SCALE) {kname}(StagedArgs a) {{ {kname}_body(a); }}"""
 
         for r, outs in enumerate(roles):
             code, _ = g.emit_role(f"{g.name}_r{r}", outs)
@@ -793,7 +793,7 @@ __device__ __forceinline__ void {kpre}_{g.tag}_r{r}_body(const StagedArgs& a) {{
     const GPair ket = a.ket[q.y];
     {fname}(bra, ket, a.prims, sboys, reinterpret_cast<{real}*>(a.acc) + tcol(t, {len(keyidx)}) + {base} * TQ, TQ);
 }}
-__global__ void __launch_bounds__(ND_THREADS, 2) {kpre}_{g.tag}_r{r}(StagedArgs a) {{ {kpre}_{g.tag}_r{r}_body(a); }}""")
+__global__ void __launch_bounds__(RB_THREADS, 2 * RB_SCALE) {kpre}_{g.tag}_r{r}(StagedArgs a) {{ {kpre}_{g.tag}_r{r}_body(a); }}""")
                 base += len(gr)
         og = prm["out_group3"]
         outroles = [list(range(i, min(i + og, g.nout))) for i in range(0, g.nout, og)]
@@ -814,7 +814,7 @@ __device__ __forceinline__ void {kname}_body(const StagedArgs& a) {{
         {fname}(bra, ket, reinterpret_cast<const {real}*>(a.acc) + tcol(t, {len(keyidx)}),
                 reinterpret_cast<{real}*>(a.out) + tcol(t, {g.nout}) + {outs[0]} * TQ, TQ);
 }}
-__global__ void __launch_bounds__(ND_THREADS) {kname}(StagedArgs a) {{ {kname}_body(a); }}""")
+__global__ void __launch_bounds__(RB_THREADS, RB_SCALE) {kname}(StagedArgs a) {{ {kname}_body(a); }}""")
         kern.append(merged_kernel(f"k_sam_{g.tag}", [f"k_sa_{g.tag}_r{r}" for r in range(len(groups))]))
         kern.append(merged_kernel(f"k_samf_{g.tag}", [f"k_saf_{g.tag}_r{r}" for r in range(len(groups32))]))
         kern.append(merged_kernel(f"k_sbm_{g.tag}", [f"k_sb_{g.tag}_r{r}" for r in range(len(outroles))], minb=1))

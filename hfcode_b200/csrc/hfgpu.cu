@@ -569,21 +569,21 @@ int run_staged_diag(hfgpu_handle* h, int t, int mode, const double* P, double th
         if (merge_roles(h, K, blocks, std::max(K.nrole_a, K.nrole_b))) {
             if (K.nrole_a > 0) {
                 ++h->launches;
-                K.ma64<<<dim3(blocks, K.nrole_a), ND_THREADS, 0, h->stream>>>(a);
+                K.ma64<<<dim3(blocks * RB_SCALE, K.nrole_a), RB_THREADS, 0, h->stream>>>(a);
                 HF_CHECK(cudaGetLastError());
             }
             ++h->launches;
-            K.mb64<<<dim3(blocks, K.nrole_b), ND_THREADS, 0, h->stream>>>(a);
+            K.mb64<<<dim3(blocks * RB_SCALE, K.nrole_b), RB_THREADS, 0, h->stream>>>(a);
             HF_CHECK(cudaGetLastError());
         } else {
             for (int r = 0; r < K.nrole_a; ++r) {
                 ++h->launches;
-                K.sa64[r]<<<blocks, ND_THREADS, 0, h->stream>>>(a);
+                K.sa64[r]<<<blocks * RB_SCALE, RB_THREADS, 0, h->stream>>>(a);
                 HF_CHECK(cudaGetLastError());
             }
             for (int r = 0; r < K.nrole_b; ++r) {
                 ++h->launches;
-                K.sb64[r]<<<blocks, ND_THREADS, 0, h->stream>>>(a);
+                K.sb64[r]<<<blocks * RB_SCALE, RB_THREADS, 0, h->stream>>>(a);
                 HF_CHECK(cudaGetLastError());
             }
         }
@@ -864,21 +864,21 @@ int run_staged(hfgpu_handle* h, int c, int prec, long long n, const double* P, d
             // a small chunk: every role of a stage in one launch, side by side
             if (na > 0) {
                 ++h->launches;
-                (prec ? K.ma32 : K.ma64)<<<dim3(blocks, na), ND_THREADS, 0, stream>>>(a);
+                (prec ? K.ma32 : K.ma64)<<<dim3(blocks * RB_SCALE, na), RB_THREADS, 0, stream>>>(a);
                 HF_CHECK(cudaGetLastError());
             }
             ++h->launches;
-            (prec ? K.mb32 : K.mb64)<<<dim3(blocks, a.nroles), ND_THREADS, 0, stream>>>(a);
+            (prec ? K.mb32 : K.mb64)<<<dim3(blocks * RB_SCALE, a.nroles), RB_THREADS, 0, stream>>>(a);
             HF_CHECK(cudaGetLastError());
         } else {
             for (int r = 0; r < na; ++r) {
                 ++h->launches;
-                (prec ? K.sa32[r] : K.sa64[r])<<<blocks, ND_THREADS, 0, stream>>>(a);
+                (prec ? K.sa32[r] : K.sa64[r])<<<blocks * RB_SCALE, RB_THREADS, 0, stream>>>(a);
                 HF_CHECK(cudaGetLastError());
             }
             for (int r = 0; r < a.nroles; ++r) {
                 ++h->launches;
-                (prec ? K.sb32[r] : K.sb64[r])<<<blocks, ND_THREADS, 0, stream>>>(a);
+                (prec ? K.sb32[r] : K.sb64[r])<<<blocks * RB_SCALE, RB_THREADS, 0, stream>>>(a);
                 HF_CHECK(cudaGetLastError());
             }
         }
